@@ -1,0 +1,290 @@
+"""CPU oracle for the FARRSIGHT per-step hot path -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries, both built by ``oracle/Makefile``:
+
+* ``oracle/_ref/libfs_ref.so`` -- the reference's own ``src/FieldStructure.cpp``
+  compiled unmodified (direct sum ``src/FieldStructure.cpp:102-156`` and treecode
+  ``:230-1020``).  This is the pin for the field.
+* ``oracle/liboracle.so`` -- ``fs_oracle.c``, a plain C restatement of the whole
+  hot path (field, treecode, panel mesh, remesh, RK4 step control).  Its field
+  functions are checked bit for bit against the reference library; the mesh /
+  remesh / RK4 parts are PARITY UNPINNED (their reference files cannot be
+  compiled here: absolute Boost include paths and Eigen).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline / reference arm
+of ``bench.py`` may import this package.  The product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(HERE, "liboracle.so")
+_REF = os.path.join(HERE, "_ref", "libfs_ref.so")
+PANEL_INTS = 18
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build(ref_dir: str | None = None) -> None:
+    """Compile the oracle (and the reference library when its sources exist)."""
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_dir:
+        cmd.append(f"REF={ref_dir}")
+    subprocess.run(cmd, check=True)
+
+
+class FsoSpecies(C.Structure):
+    _fields_ = [("q", C.c_double), ("m", C.c_double), ("initial_height", C.c_int),
+                ("p_height", C.c_int), ("pmin", C.c_double), ("pmax", C.c_double),
+                ("ics_type", C.c_int), ("pth", C.c_double), ("pstr", C.c_double),
+                ("amp", C.c_double), ("normalized_wavenumber", C.c_double)]
+
+
+class FsoSim(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("quadrature", C.c_int),
+                ("dt", C.c_double), ("remesh_period", C.c_int), ("greens_epsilon", C.c_double),
+                ("use_treecode", C.c_int), ("mac", C.c_double), ("degree", C.c_int),
+                ("max_source", C.c_int), ("num_species", C.c_int), ("species", FsoSpecies * 8)]
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        L.fso_direct_sum.argtypes = [C.c_double, C.c_double, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        L.fso_treecode.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
+        L.fso_treecode.restype = C.c_int
+        L.fso_mesh_build.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.fso_mesh_build.restype = C.c_void_p
+        L.fso_mesh_destroy.argtypes = [C.c_void_p]
+        for n in ("fso_mesh_npoints", "fso_mesh_npanels", "fso_mesh_nleaves"):
+            getattr(L, n).argtypes = [C.c_void_p]
+            getattr(L, n).restype = C.c_int
+        L.fso_mesh_points.argtypes = [C.c_void_p, _dp, _dp]
+        L.fso_mesh_panels.argtypes = [C.c_void_p, _ip]
+        L.fso_mesh_leaves.argtypes = [C.c_void_p, _ip]
+        L.fso_mesh_base_weights.argtypes = [C.c_void_p, C.c_double, C.c_int, _dp]
+        L.fso_f0.argtypes = [C.c_int] + [C.c_double] * 6
+        L.fso_f0.restype = C.c_double
+        L.fso_remesh_interp.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, _dp, _ip, _dp]
+        L.fso_remesh_interp.restype = C.c_int
+        L.fso_reduce.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _ip]
+        L.fso_reduce.restype = C.c_int
+        L.fso_sim_create.argtypes = [C.POINTER(FsoSim)]
+        L.fso_sim_create.restype = C.c_void_p
+        L.fso_sim_destroy.argtypes = [C.c_void_p]
+        L.fso_sim_step.argtypes = [C.c_void_p]
+        L.fso_sim_step.restype = C.c_int
+        L.fso_sim_total_points.argtypes = [C.c_void_p]
+        L.fso_sim_total_points.restype = C.c_int
+        L.fso_sim_species_points.argtypes = [C.c_void_p, C.c_int]
+        L.fso_sim_species_points.restype = C.c_int
+        L.fso_sim_iter.argtypes = [C.c_void_p]
+        L.fso_sim_iter.restype = C.c_int
+        L.fso_sim_state.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        L.fso_sim_counters.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF)
+
+
+def ref():
+    """The reference's own field solvers (oracle/_ref/libfs_ref.so)."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(_REF):
+            raise FileNotFoundError(f"{_REF} missing: run `make -C oracle` where the reference sources exist")
+        R = C.CDLL(_REF)
+        R.fsref_set_threads.argtypes = [C.c_int]
+        R.fsref_set_threads.restype = C.c_int
+        R.fsref_direct_sum.argtypes = [C.c_double, C.c_double, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        R.fsref_direct_sum.restype = C.c_int
+        R.fsref_treecode.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                     _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        R.fsref_treecode.restype = C.c_int
+        _ref = R
+    return _ref
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---------------------------------------------------------------- field
+def direct_sum(L, eps, targets, sources, q):
+    t, s, q = _f64(targets), _f64(sources), _f64(q)
+    es = np.zeros(len(t))
+    lib().fso_direct_sum(L, eps, es, t, len(t), s, q, len(s))
+    return es
+
+
+def treecode(L, eps, mac, degree, max_source, sources, q):
+    s, q = _f64(sources), _f64(q)
+    es = np.zeros(len(s))
+    rc = lib().fso_treecode(L, eps, mac, degree, max_source, es, s, q, len(s))
+    if rc < 0:
+        raise RuntimeError("treecode: unbounded tree recursion")
+    return es
+
+
+def ref_direct_sum(L, eps, targets, sources, q, threads=0):
+    t, s, q = _f64(targets), _f64(sources), _f64(q)
+    es = np.zeros(len(t))
+    R = ref()
+    R.fsref_set_threads(threads)
+    R.fsref_direct_sum(L, eps, es, t, len(t), s, q, len(s))
+    return es
+
+
+def ref_treecode(L, eps, mac, degree, max_source, sources, q, max_target=2000):
+    s, q = _f64(sources), _f64(q)
+    es = np.zeros(len(s))
+    ref().fsref_treecode(L, eps, mac, degree, max_source, max_target, es, s, len(s), s, q, len(s))
+    return es
+
+
+# ---------------------------------------------------------------- mesh
+class Mesh:
+    """create_prerefined_mesh + uniform refinement (AMRStructure_amr.cpp:127-230)."""
+
+    def __init__(self, h, ph, xmin, xmax, pmin, pmax):
+        self.h, self.ph = h, ph
+        self.xmin, self.xmax, self.pmin, self.pmax = xmin, xmax, pmin, pmax
+        self._m = lib().fso_mesh_build(h, ph, xmin, xmax, pmin, pmax)
+        if not self._m:
+            raise ValueError("bad mesh parameters")
+        L = lib()
+        self.npoints = L.fso_mesh_npoints(self._m)
+        self.npanels = L.fso_mesh_npanels(self._m)
+        self.nleaves = L.fso_mesh_nleaves(self._m)
+        self.xs = np.zeros(self.npoints)
+        self.ps = np.zeros(self.npoints)
+        L.fso_mesh_points(self._m, self.xs, self.ps)
+        self.panels = np.zeros((self.npanels, PANEL_INTS), dtype=np.int32)
+        L.fso_mesh_panels(self._m, self.panels)
+        self.leaves = np.zeros(self.nleaves, dtype=np.int32)
+        L.fso_mesh_leaves(self._m, self.leaves)
+
+    def base_weights(self, q, quad):
+        w = np.zeros(self.npoints)
+        lib().fso_mesh_base_weights(self._m, q, quad, w)
+        return w
+
+    def remesh(self, old_xs, old_ps, old_fs, f_beyond):
+        nf = np.zeros(self.npoints)
+        leaf = np.zeros(self.npoints, dtype=np.int32)
+        fx = np.zeros(self.npoints)
+        rc = lib().fso_remesh_interp(self._m, _f64(old_xs), _f64(old_ps), _f64(old_fs), f_beyond, nf, leaf, fx)
+        if rc:
+            raise RuntimeError("too many shifts!")
+        return nf, leaf, fx
+
+    def __del__(self):
+        if getattr(self, "_m", None):
+            lib().fso_mesh_destroy(self._m)
+            self._m = None
+
+
+def f0(ics, pth, pstr, k, amp, x, p):
+    fn = lib().fso_f0
+    return np.array([fn(ics, pth, pstr, k, amp, float(a), float(b)) for a, b in zip(x, p)])
+
+
+def reduce(xs, q):
+    xs, q = _f64(xs), _f64(q)
+    n = len(xs)
+    rx, rw, inv = np.zeros(n), np.zeros(n), np.zeros(n, dtype=np.int32)
+    u = lib().fso_reduce(xs, q, n, rx, rw, inv)
+    return rx[:u].copy(), rw[:u].copy(), inv
+
+
+# ---------------------------------------------------------------- simulation
+def sim_params(deck: dict) -> FsoSim:
+    """Deck dict (deck.json keys) -> oracle simulation parameters."""
+    P = FsoSim()
+    P.xmin, P.xmax = deck.get("xmin", 0.0), deck.get("xmax", 0.0)
+    P.quadrature = int(deck.get("quadrature", 1))
+    P.dt = deck.get("dt", 0.5)
+    P.remesh_period = int(deck.get("remesh_period", 1))
+    P.greens_epsilon = deck.get("greens_epsilon", 0.2)
+    P.use_treecode = int(deck.get("use_treecode", 0))
+    P.mac = deck.get("mac", -1.0)
+    P.degree = int(deck.get("degree", -1))
+    P.max_source = int(deck.get("max_source", 2000))
+    sl = deck["species_list"]
+    P.num_species = len(sl)
+    for i, sp in enumerate(sl):
+        S = P.species[i]
+        S.q, S.m = sp.get("q", -1.0), sp.get("m", 1.0)
+        S.initial_height, S.p_height = int(sp.get("initial_height", 6)), int(sp.get("p_height", 0))
+        S.pmin, S.pmax = sp.get("pmin", -1.0), sp.get("pmax", 1.0)
+        S.ics_type = int(sp.get("ics_type", 1))
+        S.pth, S.pstr, S.amp = sp.get("pth", 1.0), sp.get("pstr", 0.0), sp.get("amp", 0.0)
+        S.normalized_wavenumber = sp.get("normalized_wavenumber", 1.0)
+    return P
+
+
+class Sim:
+    """Oracle AMRSimulation (AMRSimulation.cpp:5-91, AMRSimulation_step.cpp:5-99)."""
+
+    def __init__(self, deck: dict):
+        self._p = sim_params(deck)
+        self._s = lib().fso_sim_create(C.byref(self._p))
+        if not self._s:
+            raise ValueError("bad deck")
+        self.n = lib().fso_sim_total_points(self._s)
+        self.species_points = [lib().fso_sim_species_points(self._s, i) for i in range(self._p.num_species)]
+
+    def step(self, n=1):
+        for _ in range(n):
+            rc = lib().fso_sim_step(self._s)
+            if rc:
+                raise RuntimeError("oracle step failed (too many shifts)")
+
+    @property
+    def iter(self):
+        return lib().fso_sim_iter(self._s)
+
+    def state(self):
+        a = {k: np.zeros(self.n) for k in ("xs", "ps", "fs", "q_ws", "es")}
+        lib().fso_sim_state(self._s, *(a[k].ctypes.data for k in ("xs", "ps", "fs", "q_ws", "es")))
+        return a
+
+    def counters(self):
+        f, r = C.c_longlong(), C.c_longlong()
+        lib().fso_sim_counters(self._s, C.byref(f), C.byref(r))
+        return f.value, r.value
+
+    def __del__(self):
+        if getattr(self, "_s", None):
+            lib().fso_sim_destroy(self._s)
+            self._s = None
+
+
+# ---------------------------------------------------------------- diagnostics
+def field_energy(xs, es, L):
+    """Field energy 0.5 * sum dx * E^2 over the unique x in [0, L) with periodic
+    centred spacing (standard_interface/diagnostic_plot.py:119-129)."""
+    xs = np.asarray(xs, dtype=np.float64)
+    es = np.asarray(es, dtype=np.float64)
+    x_sort, idx = np.unique(xs, return_index=True)
+    e_sort = es[idx]
+    keep = np.nonzero((x_sort >= 0) * (x_sort < L))
+    mx, me = x_sort[keep], e_sort[keep]
+    dxs = 0.5 * np.hstack([mx[1] + L - mx[-1], mx[2:] - mx[:-2], mx[0] + L - mx[-2]])
+    return 0.5 * float(np.dot(dxs, me ** 2))

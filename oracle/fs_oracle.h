@@ -1,0 +1,124 @@
+/* CPU oracle for the FARRSIGHT per-step hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Plain C restatement of the reference (shujhan/multi_species) algorithm.  Each
+ * function cites the reference file:line it follows.  Only tests/,
+ * __graft_entry__.smoke() and the CPU-baseline leg of bench.py may load it; the
+ * product library never links or calls it.
+ *
+ * Pinning: the field functions (fso_direct_sum, fso_treecode) are checked
+ * against the reference's own src/FieldStructure.cpp compiled unmodified into
+ * oracle/_ref/libfs_ref.so.  The mesh / remesh / RK4 / reduced-grid parts live
+ * in reference files that cannot be compiled here (they #include Boost headers
+ * by absolute path and need Eigen), so for those parts PARITY IS UNPINNED: they
+ * are a faithful restatement checked by invariants (exact quadratic
+ * reproduction, identity remesh, charge conservation) rather than by reference
+ * outputs.
+ */
+#ifndef FS_ORACLE_H
+#define FS_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- field ---------------- */
+/* E_MQ_DirectSum::operator() (src/FieldStructure.cpp:106-156). */
+void fso_direct_sum(double L, double eps, double* es, const double* targets, int nt,
+                    const double* sources, const double* q_ws, int ns);
+/* E_MQ_Treecode::operator() (src/FieldStructure.cpp:230-503); targets ignored,
+ * es[0..ns) written.  Returns the number of leaves (>0) or <0 on error. */
+int fso_treecode(double L, double eps, double mac, int degree, int max_source,
+                 double* es, const double* sources, const double* q_ws, int ns);
+
+/* ---------------- mesh ---------------- */
+/* Panel record exported as FSO_PANEL_INTS ints:
+ * [0..8] point_inds, [9] level, [10] parent, [11] which_child, [12] child_start,
+ * [13] left, [14] top, [15] right, [16] bottom,
+ * [17] flags: 1 is_left_bdry, 2 is_right_bdry, 4 is_refined_xp, 8 is_refined_p */
+#define FSO_PANEL_INTS 18
+typedef struct fso_mesh fso_mesh;
+/* create_prerefined_mesh (src/structure_files/AMRStructure_amr.cpp:127-230)
+ * with refine_panels (:506-839) and refine_panels_refine_v (:233-504),
+ * periodic boundary conditions, uniform refinement. */
+fso_mesh* fso_mesh_build(int initial_height, int p_height, double xmin, double xmax,
+                         double pmin, double pmax);
+void fso_mesh_destroy(fso_mesh* m);
+int fso_mesh_npoints(const fso_mesh* m);
+int fso_mesh_npanels(const fso_mesh* m);
+int fso_mesh_nleaves(const fso_mesh* m);
+void fso_mesh_points(const fso_mesh* m, double* xs, double* ps);
+void fso_mesh_panels(const fso_mesh* m, int* rec);
+void fso_mesh_leaves(const fso_mesh* m, int* leaf_inds);
+/* set_leaves_weights without the final *f (AMRStructure_amr.cpp:1084-1151):
+ * w[i] = sum over leaves (DFS order) of q*dx*dp/{4,9} * stencil. quad 0 trap, 1 simpson */
+void fso_mesh_base_weights(const fso_mesh* m, double q, int quad, double* w);
+
+/* ---------------- initial conditions ---------------- */
+/* src/structure_files/initial_distributions.cpp:16-140, ics_type 1,2,3,4,9,10 */
+double fso_f0(int ics_type, double pth, double pstr, double k, double amp, double x, double p);
+
+/* ---------------- remesh ---------------- */
+/* interpolate_to_initial_xps (AMRStructure_interp.cpp:493-793) with shift_xs
+ * (:429-491), the recursive first-point search (:232-426), the neighbour walk
+ * (:12-230) and the per-panel 9x9 biquadratic fit (:795-975).
+ * old_* are the deformed points of the previous mesh (same panel structure m);
+ * new_fs receives f at the mesh lattice points (in mesh point order).
+ * leaf_of_point / final_x (optional) receive the located leaf (0 = beyond the
+ * p-boundary) and the periodically shifted x used for the fit.
+ * Returns 0, or -1 when shift_xs needs more than 10 shifts (the reference throws). */
+int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old_ps,
+                      const double* old_fs, double f_beyond, double* new_fs,
+                      int* leaf_of_point, double* final_x);
+/* One 9-point biquadratic fit evaluated at (dx, dp) offsets from point 4. */
+void fso_panel_fit(const double* px, const double* py, const double* pf, int npts,
+                   const double* x, const double* p, double* out);
+
+/* ---------------- reduced grid ---------------- */
+/* get_reduced_xs_ws (src/structure_files/AMRStructure.cpp:147-185): returns the
+ * number of unique x; reduced_xs/ws sized n, inv sized n. */
+int fso_reduce(const double* xs, const double* q_ws, int n, double* reduced_xs,
+               double* reduced_ws, int* inv);
+
+/* ---------------- simulation ---------------- */
+typedef struct {
+    double q, m;
+    int initial_height, p_height;
+    double pmin, pmax;
+    int ics_type;
+    double pth, pstr, amp, normalized_wavenumber;
+} fso_species_params;
+
+typedef struct {
+    double xmin, xmax;
+    int quadrature;      /* 0 trap, 1 simpson */
+    double dt;
+    int remesh_period;
+    double greens_epsilon;
+    int use_treecode;
+    double mac;
+    int degree;
+    int max_source;
+    int num_species;
+    fso_species_params species[8];
+} fso_sim_params;
+
+typedef struct fso_sim fso_sim;
+/* AMRSimulation ctor (src/simulation_files/AMRSimulation.cpp:5-91): meshes,
+ * f0, weights, initial reduced field. */
+fso_sim* fso_sim_create(const fso_sim_params* prm);
+void fso_sim_destroy(fso_sim* s);
+/* AMRSimulation::step (src/simulation_files/AMRSimulation_step.cpp:5-99). */
+int fso_sim_step(fso_sim* s);
+int fso_sim_total_points(const fso_sim* s);
+int fso_sim_species_points(const fso_sim* s, int sp);
+int fso_sim_iter(const fso_sim* s);
+/* Concatenated state (species in deck order). Any pointer may be NULL. */
+void fso_sim_state(const fso_sim* s, double* xs, double* ps, double* fs, double* q_ws,
+                   double* es);
+/* Number of full (N x N) and reduced field evaluations done so far. */
+void fso_sim_counters(const fso_sim* s, long long* full_evals, long long* reduced_evals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
