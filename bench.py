@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark of the FARRSIGHT hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload two_stream|landau] [--field direct32c|direct64]
+
+A step is one AMRSimulation::step of the workload (RK4 with three field
+evaluations, then either the fourth field evaluation or the remesh + reduced
+grid field every 5 steps), device resident.  Default workload: the two-stream
+precision form -- 256 x 512 panels (525,825 points), eps 0.02, dt 0.2, FP32
+compensated direct sum -- with synthetic inputs generated from the deck.
+
+value     pair interactions per second over the timed steps (whole job: all
+          ranks' pairs / max-over-ranks device time), CUDA events on the
+          simulation's stream; L2 flushed (256 MiB write) between timed steps.
+e2e       same metric through the reference-facing plugin call
+          (E_MQ_DirectSum_B200.__call__, i.e. fs_field_eval with HOST arrays)
+          driving a host-side RK4 step like AMRSimulation::rk4_step: every
+          field call copies sources and weights host->device and E back.
+roofline  the pair kernel (k_pairs32): achieved pair rate per launch-time
+          against the MUFU reciprocal-square-root peak (one MUFU op per pair).
+cpu_baseline  the reference's own E_MQ_DirectSum (oracle/_ref, compiled from
+          the reference sources) on all host cores, on a bounded target sample.
+
+Multi-GPU: replicas only (one independent simulation per rank, no data-path
+collective); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MUFU_RSQ_PER_CLK_PER_SM = 16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="two_stream", choices=["two_stream", "landau"])
+    ap.add_argument("--field", default="direct32c", choices=["direct32c", "direct64"])
+    ap.add_argument("--h", type=int, default=None, help="override the mesh height (small cases for profiling)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload_deck(a):
+    from multi_species_b200 import decks
+    if a.workload == "two_stream":
+        d = decks.two_stream(h=a.h or 8, ph=1, steps=100, remesh_period=5)
+        name = "two_stream_precision_form"
+    else:
+        d = decks.landau_two_species(h=a.h or 5, ph=1)
+        name = "landau_two_species"
+    return name, d
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clock, throttle reasons)."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def traffic_per_pair(kernel: str):
+    """DRAM bytes per pair of the pair kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(deck, seconds: float):
+    """Reference E_MQ_DirectSum on all host cores over a sample of targets."""
+    import oracle as O
+    import multi_species_b200 as M
+    sp = deck["species_list"][0]
+    m = M.mesh(sp["initial_height"], sp["p_height"], deck["xmin"], deck["xmax"], sp["pmin"], sp["pmax"],
+               q=sp["q"], quadrature=deck["quadrature"])
+    x = m["xs"] + 0.2 * m["ps"]
+    q = m["base_weights"]
+    L = deck["xmax"] - deck["xmin"]
+    cores = os.cpu_count() or 1
+    nt = 256
+    while True:
+        t0 = time.perf_counter()
+        O.ref_direct_sum(L, deck["greens_epsilon"], x[:nt], x, q, threads=cores)
+        dt = time.perf_counter() - t0
+        if dt > 0.5 or nt >= len(x):
+            break
+        nt = min(len(x), nt * 4)
+    nt = int(min(len(x), max(nt, nt * seconds / max(dt, 1e-9) / 2)))
+    t0 = time.perf_counter()
+    O.ref_direct_sum(L, deck["greens_epsilon"], x[:nt], x, q, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": nt * len(x) / dt, "unit": "pair-interactions/s", "cores": cores, "kind": "reference",
+            "sample": f"{nt} targets x {len(x)} sources of the workload's point set, one field evaluation "
+                      f"({dt:.1f} s)"}
+
+
+def run_reference(a, rank, world):
+    """--impl reference: the reference's CPU direct sum on the host cores."""
+    name, deck = workload_deck(a)
+    if rank != 0:
+        return None
+    vals = []
+    per = max(1.0, a.cpu_seconds / max(1, a.steps + a.warmup))
+    for _ in range(a.warmup):
+        cpu_baseline(deck, per)
+    for _ in range(a.steps):
+        vals.append(cpu_baseline(deck, per))
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    return {"metric": "pair-interactions/s", "value": v, "unit": "pair-interactions/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (deck-generated point set)",
+            "impl": "reference",
+            "config": {"workload": name, "points": None, "field": "reference E_MQ_DirectSum (CPU, OpenMP)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def host_rk4_step(field, xs, ps, es, qw, qm, dt):
+    """AMRSimulation::rk4_step + end-of-step field on the host, each field
+    evaluation through the plugin call with host arrays."""
+    n = len(xs)
+    ef1 = es * qm
+    p2 = ps + 0.5 * dt * ef1
+    xk = xs + 0.5 * dt * ps
+    ef2 = np.empty(n)
+    field(ef2, xk, n, xk, qw, n)
+    ef2 *= qm
+    p3 = ps + 0.5 * dt * ef2
+    xk = xs + 0.5 * dt * p2
+    ef3 = np.empty(n)
+    field(ef3, xk, n, xk, qw, n)
+    ef3 *= qm
+    p4 = ps + dt * ef3
+    xk = xs + dt * p3
+    ef4 = np.empty(n)
+    field(ef4, xk, n, xk, qw, n)
+    ef4 *= qm
+    xs = xs + dt / 6.0 * (ps + 2 * p2 + 2 * p3 + p4)
+    ps = ps + dt / 6.0 * (ef1 + 2 * ef2 + 2 * ef3 + ef4)
+    es = np.empty(n)
+    field(es, xs, n, xs, qw, n)
+    return xs, ps, es
+
+
+def run_ours(a, rank, world, local_rank):
+    import multi_species_b200 as M
+    import torch
+    name, deck = workload_deck(a)
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    sim = M.Simulation(deck, field_backend=a.field, device=local_rank)
+    n = sim.n
+    for _ in range(a.warmup):
+        sim.step(1)
+    M.profile_reset()
+    M.profile_enable(True)
+    launches0 = M.kernel_launches()
+    pairs0 = sim.pair_count()
+    step_ms = []
+    dist = world > 1
+    if dist:
+        import torch.distributed as D
+        D.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sim.step(1)
+            step_ms.extend(sim.step_times().tolist())
+    torch.cuda.synchronize()
+    if dist:
+        D.barrier()
+    M.profile_enable(False)
+    launches = M.kernel_launches() - launches0
+    pairs = sim.pair_count() - pairs0
+    total_ms = float(np.sum(step_ms))
+    kern = "k_pairs32" if a.field == "direct32c" else "k_direct64"
+    kl, kms, kwork = M.profile_read(kern)
+    rl, rms, _ = M.profile_read("remesh")
+    t_max = total_ms
+    pairs_all = pairs
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        t_max = float(t.item())
+        pw = torch.tensor([pairs], dtype=torch.float64)
+        D.all_reduce(pw, op=D.ReduceOp.SUM)
+        pairs_all = float(pw.item())
+    value = pairs_all / (t_max / 1e3)
+    res = None
+    if rank == 0:
+        peaks, peak_src = measured_peaks()
+        sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        clocks = clk.summary()
+        mhz = float(peaks.get("sm_max_mhz", 1965.0))
+        peak = sm * MUFU_RSQ_PER_CLK_PER_SM * mhz * 1e6
+        achieved = kwork / (kms / 1e3) if kms > 0 else 0.0
+        tr = traffic_per_pair(kern)
+        roof = {"kernel": kern, "bound": "mufu", "unit": "Gpair/s", "achieved": achieved / 1e9, "peak": peak / 1e9,
+                "frac": achieved / peak if peak else None,
+                "peak_source": f"{sm} SMs x {MUFU_RSQ_PER_CLK_PER_SM} MUFU rsqrt/clk x sm_max_mhz {mhz:.0f} "
+                               f"({peak_src} MEASURED_PEAKS.json clock); one rsqrt per pair",
+                "launches": kl, "avg_launch_ms": kms / kl if kl else None,
+                "pairs_per_launch": kwork / kl if kl else None,
+                "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
+                "kernel_share_of_step_time": kms / total_ms if total_ms else None}
+        if a.field == "direct64":
+            roof["bound"] = "fp64"
+        res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
+               "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if a.field == "direct32c" else "f64",
+               "data": "synthetic (deck-generated, no dataset)",
+               "config": {"workload": name, "points": n, "field": a.field, "eps": deck["greens_epsilon"],
+                          "dt": deck["dt"], "remesh_period": deck["remesh_period"], "parallelism": f"replicas{world}",
+                          "l2": "flushed (256 MiB write) between timed steps"},
+               "rk4_steps_per_s": a.steps / (t_max / 1e3) * world,
+               "remesh_ms_per_remesh": (rms / rl) if rl else None,
+               "gpu_launches": int(launches), "roofline": roof, "clocks": clocks}
+        if not a.no_e2e:
+            res["e2e"] = e2e_plugin(deck, a.field, n, local_rank)
+        if not a.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(deck, a.cpu_seconds)
+    sim.close()
+    return res
+
+
+def e2e_plugin(deck, field_kind, n, device):
+    import multi_species_b200 as M
+    sim = M.Simulation(deck, field_backend=field_kind, device=device)
+    st = sim.state()
+    sim.close()
+    L = deck["xmax"] - deck["xmin"]
+    f = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], "fp32c" if field_kind == "direct32c" else "fp64",
+                              device=device)
+    sp = deck["species_list"][0]
+    qm = sp["q"] / sp["m"]
+    xs, ps, es, qw = st["xs"], st["ps"], st["es"], st["q_ws"]
+    xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"])  # warm-up
+    steps = 2
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"])
+    dt = time.perf_counter() - t0
+    f.close()
+    pairs = 4.0 * n * n * steps
+    return {"value": pairs / dt, "unit": "pair-interactions/s", "h2d_bytes_per_step": 4 * 16 * n,
+            "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
+            "path": "E_MQ_DirectSum_B200(es, targets, nt, sources, q_ws, ns) with host arrays, host RK4"}
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as D
+        D.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    try:
+        if a.impl == "reference":
+            res = run_reference(a, rank, world)
+        else:
+            res = run_ours(a, rank, world, local_rank)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as D
+            D.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+/* fs_b200.h -- C ABI of the B200 (sm_100a) FARRSIGHT hot path.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an fs_status
+ * (0 = FS_OK); fs_last_error() gives a message for the calling thread.
+ *
+ * Reference interfaces replaced (shujhan/multi_species):
+ *   ElectricField::operator()(es, targets, nt, sources, q_ws, ns)
+ *       inc/FieldStructure.hpp:87-93, implementations E_MQ_DirectSum
+ *       src/FieldStructure.cpp:106-156 and E_MQ_Treecode :230-503
+ *       -> fs_field_create / fs_field_eval / fs_field_eval_device
+ *   AMRSimulation::step / rk4_step / remesh / evaluate_field(_uniform_grid)
+ *       inc/AMRSimulation.hpp:113-127, src/simulation_files/AMRSimulation_step.cpp:5-263,
+ *       AMRSimulation_remesh.cpp:3-48, AMRSimulation_field.cpp:5-173
+ *       -> fs_sim_create / fs_sim_step / fs_sim_export
+ *   AMRStructure::create_prerefined_mesh / set_leaves_weights
+ *       src/structure_files/AMRStructure_amr.cpp:127-230, :1084-1151
+ *       -> fs_mesh_sizes / fs_mesh_fill (host only, no GPU needed)
+ */
+#ifndef FS_B200_H
+#define FS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fs_status {
+    FS_OK = 0,
+    FS_ERR_ARG = 1,          /* invalid argument                                  */
+    FS_ERR_CUDA = 2,         /* CUDA runtime error                                 */
+    FS_ERR_NOMEM = 3,        /* device allocation failed / over the HBM budget     */
+    FS_ERR_WALK = 4,         /* remesh point location did not converge (bounded)   */
+    FS_ERR_SHIFT = 5,        /* remesh periodic shift needed > 10 shifts           */
+    FS_ERR_TIMEOUT = 6,      /* a bounded device wait gave up                      */
+    FS_ERR_STATE = 7,        /* call not valid in the current state                */
+    FS_ERR_UNSUPPORTED = 8,  /* option not supported (e.g. open boundaries)        */
+    FS_ERR_TREE = 9          /* treecode: tree deeper than the supported bound     */
+} fs_status;
+
+/* Field solver kind.  DIRECT64 is the reference arithmetic in FP64 (bit-exact
+ * with E_MQ_DirectSum); DIRECT32C is the FP32 pair kernel with compensation and
+ * FP64 background; TREECODE64 / TREECODE32C are the barycentric Lagrange
+ * treecode of E_MQ_Treecode with an FP64 / FP32-compensated near field. */
+typedef enum fs_field_kind {
+    FS_FIELD_DIRECT64 = 0,
+    FS_FIELD_DIRECT32C = 1,
+    FS_FIELD_TREECODE64 = 2,
+    FS_FIELD_TREECODE32C = 3
+} fs_field_kind;
+
+/* Parameters of AMRSimulation::make_field_return_ptr
+ * (src/simulation_files/AMRSimulation_load.cpp:49-96). */
+typedef struct fs_field_params {
+    double L;          /* Lx = x_max - x_min (periodic)          */
+    double epsilon;    /* greens_epsilon                         */
+    int kind;          /* fs_field_kind                          */
+    double mac;        /* treecode MAC theta                     */
+    int degree;        /* treecode interpolation degree (<= 16)  */
+    int max_source;    /* treecode leaf size                     */
+    int max_target;    /* accepted and ignored, as in the reference */
+    int device;        /* CUDA device ordinal                    */
+} fs_field_params;
+
+typedef struct fs_field fs_field;
+
+fs_status fs_field_create(const fs_field_params* params, fs_field** out);
+fs_status fs_field_destroy(fs_field* field);
+
+/* ElectricField::operator() drop-in (inc/FieldStructure.hpp:87-93): host
+ * arrays, synchronous.  Fully overwrites es[0..nt).  For the treecode kinds the
+ * reference ignores targets/nt and writes es[0..ns); so does this call
+ * (nt must equal ns). */
+fs_status fs_field_eval(fs_field* field, double* es, const double* targets, int nt,
+                        const double* sources, const double* q_ws, int ns);
+
+/* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
+ * the field's own stream); returns without synchronising. */
+fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_targets, int nt,
+                               const double* d_sources, const double* d_q_ws, int ns,
+                               void* stream);
+
+/* ------------------------------------------------------------------ session */
+/* One species of the deck (AMRSimulation_load.cpp:188-270 keys). */
+typedef struct fs_species_params {
+    double q, m;
+    int initial_height, p_height;
+    double pmin, pmax;
+    int ics_type;                 /* 1,2 Landau; 3 strong two-stream; 4 colder two-stream; 9,10 ion acoustic */
+    double pth, pstr, amp, normalized_wavenumber;
+} fs_species_params;
+
+/* Deck-level parameters (AMRSimulation_load.cpp:14-47). */
+typedef struct fs_sim_params {
+    double xmin, xmax;
+    int quadrature;               /* 0 trapezoid, 1 Simpson                     */
+    double dt;
+    int remesh_period;
+    double greens_epsilon;
+    int field_kind;               /* fs_field_kind                              */
+    double mac;
+    int degree;
+    int max_source;
+    int num_species;              /* 1..8                                       */
+    fs_species_params species[8];
+    int device;
+} fs_sim_params;
+
+typedef struct fs_sim fs_sim;
+
+/* AMRSimulation ctor (src/simulation_files/AMRSimulation.cpp:5-91): builds the
+ * meshes on the host, f0 and weights, uploads the state and evaluates the
+ * initial reduced-grid field on the device. */
+fs_status fs_sim_create(const fs_sim_params* params, fs_sim** out);
+fs_status fs_sim_destroy(fs_sim* sim);
+/* nsteps x AMRSimulation::step (AMRSimulation_step.cpp:5-99), device resident,
+ * synchronous on return. */
+fs_status fs_sim_step(fs_sim* sim, int nsteps);
+/* AMRSimulation::remesh (AMRSimulation_remesh.cpp:3-48) on the current state:
+ * every species is interpolated onto its fresh mesh and the reduced-grid field
+ * is evaluated.  fs_sim_step calls it every remesh_period steps. */
+fs_status fs_sim_remesh(fs_sim* sim);
+/* Total points (species = -1) or the points of one species. */
+fs_status fs_sim_num_points(const fs_sim* sim, int species, int* n);
+/* Copy the concatenated state (species in deck order) to host arrays; any
+ * pointer may be NULL (AMRSimulation::scatter / write_to_file). */
+fs_status fs_sim_export(fs_sim* sim, double* xs, double* ps, double* fs, double* q_ws, double* es);
+/* Overwrite positions/velocities of the current state from host arrays (for
+ * tests that inject a given state; weights and f are kept). */
+fs_status fs_sim_import_xp(fs_sim* sim, const double* xs, const double* ps, const double* es);
+fs_status fs_sim_iter(const fs_sim* sim, int* iter, double* t);
+/* Pair interactions evaluated so far (full + reduced), for throughput metrics. */
+fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs);
+
+/* ------------------------------------------------------------- host mesh */
+/* Sizes of the uniform periodic panel mesh of create_prerefined_mesh. */
+fs_status fs_mesh_sizes(int initial_height, int p_height, int* npoints, int* npanels, int* nleaves);
+/* Fill points (reference point order), panels (18 ints each: point_inds[9],
+ * level, parent, which_child, child_start, left, top, right, bottom, flags
+ * 1 left-bdry 2 right-bdry 4 refined-xp 8 refined-p), leaves (DFS order) and
+ * base quadrature weights q*dx*dp*stencil (before the *f of set_leaves_weights).
+ * Any output pointer may be NULL. */
+fs_status fs_mesh_fill(int initial_height, int p_height, double xmin, double xmax, double pmin,
+                       double pmax, double q, int quadrature, double* xs, double* ps, int* panels,
+                       int* leaves, double* base_weights);
+
+/* Device time of each step of the last fs_sim_step call, in ms, measured with
+ * CUDA events on the simulation's stream; *n receives the count (<= cap). */
+fs_status fs_sim_step_times(const fs_sim* sim, double* ms, int cap, int* n);
+
+/* ------------------------------------------------------------- profiling */
+/* When enabled, the library brackets its dominant kernels (pair kernels,
+ * treecode near/far kernels, remesh kernels) with CUDA events on the stream
+ * they are launched on.  fs_profile_read synchronises on the pending events and
+ * returns the launches, summed device time and summed algorithmic work (pair
+ * interactions for field kernels) of kernels named `kernel` (e.g.
+ * "k_pairs32", "k_direct64", "remesh"). */
+fs_status fs_profile_enable(int on);
+fs_status fs_profile_read(const char* kernel, long long* launches, double* total_ms, double* total_work);
+fs_status fs_profile_reset(void);
+
+/* ------------------------------------------------------------- misc */
+const char* fs_last_error(void);
+int fs_version(void);
+/* Kernels launched by this library in this process so far. */
+long long fs_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FS_B200_H */

@@ -1,0 +1,337 @@
+"""B200 (sm_100a) implementation of the FARRSIGHT per-step hot path.
+
+Python mirror of the reference's operator interfaces over the C ABI of
+``libfs_b200.so`` (declared in ``include/fs_b200.h``):
+
+* ``E_MQ_DirectSum_B200`` / ``E_MQ_Treecode_B200`` -- drop-ins for the
+  reference's ``ElectricField`` subclasses (``inc/FieldStructure.hpp:87-198``):
+  ``field(es, targets, nt, sources, q_ws, ns)`` fills ``es`` exactly like
+  ``ElectricField::operator()``; ``field.evaluate(targets, sources, q_ws)``
+  returns a new array.
+* ``Simulation`` -- the device-resident ``AMRSimulation``
+  (``inc/AMRSimulation.hpp:63-131``): ``step()``, ``run()``, ``state()``.
+* ``mesh(...)`` -- the host panel mesh of ``create_prerefined_mesh``.
+
+There is no CPU fallback: if the CUDA library is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfs_b200.so")
+
+FS_FIELD_DIRECT64 = 0
+FS_FIELD_DIRECT32C = 1
+FS_FIELD_TREECODE64 = 2
+FS_FIELD_TREECODE32C = 3
+PANEL_INTS = 18
+
+STATUS = {0: "FS_OK", 1: "FS_ERR_ARG", 2: "FS_ERR_CUDA", 3: "FS_ERR_NOMEM", 4: "FS_ERR_WALK",
+          5: "FS_ERR_SHIFT", 6: "FS_ERR_TIMEOUT", 7: "FS_ERR_STATE", 8: "FS_ERR_UNSUPPORTED",
+          9: "FS_ERR_TREE"}
+
+# Every symbol include/fs_b200.h declares (checked by the tests).
+EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
+           "fs_sim_create", "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export",
+           "fs_sim_import_xp", "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes",
+           "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
+           "fs_version", "fs_kernel_launches"]
+
+
+class FsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class FieldParams(C.Structure):
+    _fields_ = [("L", C.c_double), ("epsilon", C.c_double), ("kind", C.c_int), ("mac", C.c_double),
+                ("degree", C.c_int), ("max_source", C.c_int), ("max_target", C.c_int), ("device", C.c_int)]
+
+
+class SpeciesParams(C.Structure):
+    _fields_ = [("q", C.c_double), ("m", C.c_double), ("initial_height", C.c_int), ("p_height", C.c_int),
+                ("pmin", C.c_double), ("pmax", C.c_double), ("ics_type", C.c_int), ("pth", C.c_double),
+                ("pstr", C.c_double), ("amp", C.c_double), ("normalized_wavenumber", C.c_double)]
+
+
+class SimParams(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("quadrature", C.c_int), ("dt", C.c_double),
+                ("remesh_period", C.c_int), ("greens_epsilon", C.c_double), ("field_kind", C.c_int),
+                ("mac", C.c_double), ("degree", C.c_int), ("max_source", C.c_int), ("num_species", C.c_int),
+                ("species", SpeciesParams * 8), ("device", C.c_int)]
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def lib():
+    """Load libfs_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m multi_species_b200.build` "
+                              "(the CUDA library is required; there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        st = C.c_int
+        L.fs_field_create.argtypes = [C.POINTER(FieldParams), C.POINTER(C.c_void_p)]
+        L.fs_field_destroy.argtypes = [C.c_void_p]
+        L.fs_field_eval.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        L.fs_field_eval_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                           C.c_int, C.c_void_p]
+        L.fs_sim_create.argtypes = [C.POINTER(SimParams), C.POINTER(C.c_void_p)]
+        L.fs_sim_destroy.argtypes = [C.c_void_p]
+        L.fs_sim_step.argtypes = [C.c_void_p, C.c_int]
+        L.fs_sim_remesh.argtypes = [C.c_void_p]
+        L.fs_sim_num_points.argtypes = [C.c_void_p, C.c_int, _ip]
+        L.fs_sim_export.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.fs_sim_import_xp.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.fs_sim_iter.argtypes = [C.c_void_p, _ip, _dp]
+        L.fs_sim_pair_count.argtypes = [C.c_void_p, _dp]
+        L.fs_sim_step_times.argtypes = [C.c_void_p, _dp, C.c_int, _ip]
+        L.fs_profile_enable.argtypes = [C.c_int]
+        L.fs_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), _dp, _dp]
+        L.fs_profile_reset.argtypes = []
+        L.fs_mesh_sizes.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
+        L.fs_mesh_fill.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, _dp, _dp, _ip, _ip, _dp]
+        for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device", "fs_sim_create",
+                  "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export", "fs_sim_import_xp",
+                  "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes", "fs_mesh_fill",
+                  "fs_profile_enable", "fs_profile_read", "fs_profile_reset"):
+            getattr(L, n).restype = st
+        L.fs_last_error.restype = C.c_char_p
+        L.fs_version.restype = C.c_int
+        L.fs_kernel_launches.restype = C.c_longlong
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise FsError(rc, lib().fs_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def kernel_launches() -> int:
+    return int(lib().fs_kernel_launches())
+
+
+def profile_enable(on: bool = True) -> None:
+    _check(lib().fs_profile_enable(1 if on else 0))
+
+
+def profile_reset() -> None:
+    _check(lib().fs_profile_reset())
+
+
+def profile_read(kernel: str):
+    """(launches, total device ms, total work) of the named kernel since the last reset."""
+    n, ms, w = C.c_longlong(), C.c_double(), C.c_double()
+    _check(lib().fs_profile_read(kernel.encode(), C.byref(n), C.byref(ms), C.byref(w)))
+    return n.value, ms.value, w.value
+
+
+# --------------------------------------------------------------------- field
+class _Field:
+    kind = FS_FIELD_DIRECT64
+
+    def __init__(self, L: float, epsilon: float, kind: int, mac=-1.0, degree=-1, max_source=2000,
+                 max_target=2000, device=0):
+        self.L, self.epsilon = float(L), float(epsilon)
+        p = FieldParams(float(L), float(epsilon), int(kind), float(mac), int(degree), int(max_source),
+                        int(max_target), int(device))
+        h = C.c_void_p()
+        _check(lib().fs_field_create(C.byref(p), C.byref(h)))
+        self._h = h
+
+    def __call__(self, es, targets, nt, sources, q_ws, ns):
+        """ElectricField::operator()(es, targets, nt, sources, q_ws, ns): fills es in place."""
+        for a in (es, targets, sources, q_ws):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TypeError("arrays must be C-contiguous float64 numpy arrays")
+        _check(lib().fs_field_eval(self._h, _ptr(es), _ptr(targets), int(nt), _ptr(sources), _ptr(q_ws), int(ns)))
+
+    def evaluate(self, targets, sources, q_ws):
+        t, s, q = _f64(targets), _f64(sources), _f64(q_ws)
+        es = np.zeros(len(t))
+        self(es, t, len(t), s, q, len(s))
+        return es
+
+    def evaluate_device(self, d_es, d_targets, nt, d_sources, d_q, ns, stream=None):
+        """Device-pointer variant (integers: CUDA device addresses)."""
+        _check(lib().fs_field_eval_device(self._h, d_es, d_targets, nt, d_sources, d_q, ns, stream))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fs_field_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class E_MQ_DirectSum_B200(_Field):
+    """E_MQ_DirectSum(L, epsilon) (src/FieldStructure.cpp:102-164) on the GPU.
+
+    precision="fp64": the reference arithmetic, bit-identical results.
+    precision="fp32c": FP32 pair kernel with compensation + FP64 background.
+    """
+
+    def __init__(self, L, epsilon, precision="fp64", device=0):
+        kind = {"fp64": FS_FIELD_DIRECT64, "fp32c": FS_FIELD_DIRECT32C}[precision]
+        super().__init__(L, epsilon, kind, device=device)
+
+
+class E_MQ_Treecode_B200(_Field):
+    """E_MQ_Treecode(L, epsilon, mac, degree, max_source, max_target, verbosity)
+    (src/FieldStructure.cpp:210-503) on the GPU.  Like the reference it ignores
+    the targets and evaluates at the sources."""
+
+    def __init__(self, L, epsilon, mac, degree, max_source, max_target=2000, verbosity=0, precision="fp64",
+                 device=0):
+        kind = {"fp64": FS_FIELD_TREECODE64, "fp32c": FS_FIELD_TREECODE32C}[precision]
+        super().__init__(L, epsilon, kind, mac, degree, max_source, max_target, device=device)
+
+
+# --------------------------------------------------------------------- simulation
+FIELD_KINDS = {"direct64": FS_FIELD_DIRECT64, "direct32c": FS_FIELD_DIRECT32C, "treecode64": FS_FIELD_TREECODE64,
+               "treecode32c": FS_FIELD_TREECODE32C}
+
+
+def sim_params(deck: dict, field_backend: str | None = None, device: int = 0) -> SimParams:
+    """deck.json keys (src/simulation_files/AMRSimulation_load.cpp:14-270) -> SimParams.
+    `field_backend` (or the deck's optional "field_backend" key) picks the solver;
+    the default follows use_treecode like make_field_return_ptr."""
+    if int(deck.get("bcs", 0)) != 0:
+        raise FsError(8, "only periodic boundary conditions (bcs=0) are implemented")
+    P = SimParams()
+    P.xmin, P.xmax = float(deck.get("xmin", 0.0)), float(deck.get("xmax", 0.0))
+    P.quadrature = int(deck.get("quadrature", 1))
+    P.dt = float(deck.get("dt", 0.5))
+    P.remesh_period = int(deck.get("remesh_period", 1))
+    P.greens_epsilon = float(deck.get("greens_epsilon", 0.2))
+    backend = field_backend or deck.get("field_backend")
+    if backend is None:
+        backend = "treecode64" if int(deck.get("use_treecode", 0)) > 0 else "direct64"
+    P.field_kind = FIELD_KINDS[backend]
+    P.mac = float(deck.get("mac", -1.0))
+    P.degree = int(deck.get("degree", -1))
+    P.max_source = int(deck.get("max_source", 2000))
+    sl = deck["species_list"]
+    if not 1 <= len(sl) <= 8:
+        raise FsError(1, "species_list must hold 1..8 species")
+    P.num_species = len(sl)
+    for i, sp in enumerate(sl):
+        S = P.species[i]
+        S.q, S.m = float(sp.get("q", -1.0)), float(sp.get("m", 1.0))
+        S.initial_height, S.p_height = int(sp.get("initial_height", 6)), int(sp.get("p_height", 0))
+        S.pmin, S.pmax = float(sp.get("pmin", -1.0)), float(sp.get("pmax", 1.0))
+        S.ics_type = int(sp.get("ics_type", 1))
+        S.pth, S.pstr, S.amp = float(sp.get("pth", 1.0)), float(sp.get("pstr", 0.0)), float(sp.get("amp", 0.0))
+        S.normalized_wavenumber = float(sp.get("normalized_wavenumber", 1.0))
+    P.device = int(device)
+    return P
+
+
+class Simulation:
+    """Device-resident AMRSimulation (inc/AMRSimulation.hpp:63-131)."""
+
+    def __init__(self, deck: dict, field_backend: str | None = None, device: int = 0):
+        self.deck = deck
+        self._p = sim_params(deck, field_backend, device)
+        h = C.c_void_p()
+        _check(lib().fs_sim_create(C.byref(self._p), C.byref(h)))
+        self._h = h
+        n = C.c_int()
+        _check(lib().fs_sim_num_points(self._h, -1, C.byref(n)))
+        self.n = n.value
+        self.species_points = []
+        for s in range(self._p.num_species):
+            _check(lib().fs_sim_num_points(self._h, s, C.byref(n)))
+            self.species_points.append(n.value)
+        self.num_steps = int(deck.get("num_steps", 10))
+
+    def step(self, n: int = 1) -> None:
+        """n x AMRSimulation::step (AMRSimulation_step.cpp:5-99)."""
+        _check(lib().fs_sim_step(self._h, int(n)))
+
+    def remesh(self) -> None:
+        """AMRSimulation::remesh (AMRSimulation_remesh.cpp:3-48) on the current state."""
+        _check(lib().fs_sim_remesh(self._h))
+
+    def run(self) -> None:
+        """AMRSimulation::run (AMRSimulation_run.cpp:3-10)."""
+        it, _ = self.iteration()
+        if it < self.num_steps:
+            self.step(self.num_steps - it)
+
+    def iteration(self):
+        i, t = C.c_int(), C.c_double()
+        _check(lib().fs_sim_iter(self._h, C.byref(i), C.byref(t)))
+        return i.value, t.value
+
+    def step_times(self):
+        """Device ms of each step of the last step() call (CUDA events on the sim stream)."""
+        buf = np.zeros(4096)
+        n = C.c_int()
+        _check(lib().fs_sim_step_times(self._h, _ptr(buf), len(buf), C.byref(n)))
+        return buf[: n.value].copy()
+
+    def pair_count(self) -> float:
+        v = C.c_double()
+        _check(lib().fs_sim_pair_count(self._h, C.byref(v)))
+        return v.value
+
+    def state(self) -> dict:
+        a = {k: np.zeros(self.n) for k in ("xs", "ps", "fs", "q_ws", "es")}
+        _check(lib().fs_sim_export(self._h, *(_ptr(a[k]) for k in ("xs", "ps", "fs", "q_ws", "es"))))
+        return a
+
+    def import_xp(self, xs=None, ps=None, es=None) -> None:
+        arrs = [None if v is None else _f64(v) for v in (xs, ps, es)]
+        for v in arrs:
+            if v is not None and len(v) != self.n:
+                raise ValueError("length mismatch")
+        _check(lib().fs_sim_import_xp(self._h, *(_ptr(v) for v in arrs)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fs_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------- host mesh
+def mesh(initial_height, p_height, xmin, xmax, pmin, pmax, q=-1.0, quadrature=0):
+    """Uniform periodic panel mesh (create_prerefined_mesh, AMRStructure_amr.cpp:127-230),
+    built by the library's host code.  Returns dict of xs, ps, panels (n x 18), leaves, base_weights."""
+    npts, npan, nlv = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().fs_mesh_sizes(initial_height, p_height, C.byref(npts), C.byref(npan), C.byref(nlv)))
+    xs, ps, w = np.zeros(npts.value), np.zeros(npts.value), np.zeros(npts.value)
+    panels = np.zeros((npan.value, PANEL_INTS), dtype=np.int32)
+    leaves = np.zeros(nlv.value, dtype=np.int32)
+    _check(lib().fs_mesh_fill(initial_height, p_height, xmin, xmax, pmin, pmax, q, quadrature, _ptr(xs), _ptr(ps),
+                              panels.ctypes.data_as(_ip), leaves.ctypes.data_as(_ip), _ptr(w)))
+    return {"xs": xs, "ps": ps, "panels": panels, "leaves": leaves, "base_weights": w}

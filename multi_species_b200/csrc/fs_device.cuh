@@ -1,0 +1,70 @@
+// Device helpers shared by the kernels of libfs_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fs_internal.h"
+
+namespace fsb {
+
+// FP64 arithmetic with one rounding per operation.  The reference is plain C++
+// compiled without fused multiply-adds; using these (never contracted)
+// intrinsics everywhere a bit-identical FP64 result is claimed keeps the device
+// arithmetic the same as the reference's, whatever -fmad says.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ __forceinline__ double stage_qm(const Stage& S, int o) {
+    double qm = S.qm[0];
+#pragma unroll
+    for (int s = 1; s < 8; ++s)
+        if (s < S.nsp && o >= S.start[s]) qm = S.qm[s];
+    return qm;
+}
+
+// RK4 epilogue for point o given the raw field E at that point
+// (src/simulation_files/AMRSimulation_step.cpp:178-248).
+__device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
+    switch (S.kind) {
+        case STAGE_STORE:
+            S.out[o] = E;
+            break;
+        case STAGE_RK2: {
+            const double ef = dmul(E, stage_qm(S, o));
+            const double p2 = S.pst[o];
+            S.xk[o] = dadd(S.x[o], dmul(S.hdt, p2));
+            S.accX[o] = dadd(S.accX[o], dmul(2.0, p2));
+            S.accP[o] = dadd(S.accP[o], dmul(2.0, ef));
+            S.pst[o] = dadd(S.p[o], dmul(S.hdt, ef));  // p3
+            break;
+        }
+        case STAGE_RK3: {
+            const double ef = dmul(E, stage_qm(S, o));
+            const double p3 = S.pst[o];
+            S.xk[o] = dadd(S.x[o], dmul(S.dt, p3));
+            S.accX[o] = dadd(S.accX[o], dmul(2.0, p3));
+            S.accP[o] = dadd(S.accP[o], dmul(2.0, ef));
+            S.pst[o] = dadd(S.p[o], dmul(S.dt, ef));  // p4
+            break;
+        }
+        case STAGE_RK4: {
+            const double ef = dmul(E, stage_qm(S, o));
+            const double p4 = S.pst[o];
+            const double ax = dadd(S.accX[o], p4);
+            const double ap = dadd(S.accP[o], ef);
+            S.x[o] = dadd(S.x[o], dmul(S.dt6, ax));
+            S.p[o] = dadd(S.p[o], dmul(S.dt6, ap));
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// Bounded spin limit for every device-side wait (mbarrier, flags).
+constexpr long long kSpinLimit = 1LL << 26;
+
+}  // namespace fsb

@@ -1,0 +1,442 @@
+// FP32 compensated periodic direct sum (sm_100a).
+//
+// Same field as E_MQ_DirectSum (src/FieldStructure.cpp:106-156), rewritten as
+//   E_i = sum_j q_j g(d_ij) - c * sum_j q_j d_ij,   g(d) = d / (2 sqrt(d^2 + eps^2)),
+//   d_ij = x_i - x_j wrapped into [-L/2, L/2],       c = 1 / sqrt(L^2 + 4 eps^2).
+// The second (neutralising-background) term is linear in d and is evaluated
+// exactly in FP64 from prefix sums over the x-sorted sources.  Only g is
+// evaluated per pair, in FP32:
+//
+//  * Sources are wrapped into [0, L), sorted by x and cut into tiles of kS.
+//    Each tile stores FP32 offsets s_j = x_j - b_t from an FP64 tile base b_t,
+//    and q_j/2.  Per (target, tile) the target offset tau = x_i + shift - b_t
+//    is formed in FP64 and rounded once, so d = tau - s_j is accurate to the
+//    tile's scale, not to L.
+//  * The periodic image of every pair is fixed by one index J_i per target
+//    (sources before / after J_i take one of two images); the FP64 background
+//    term uses the same split, so both halves of the kernel agree exactly on
+//    which image a pair uses.
+//  * For a tile lying wholly on one side of the target (sigma = +-1) the pair
+//    kernel accumulates q/2 * (d*y - sigma) and adds sigma * sum(q/2) in FP64
+//    afterwards; the accumulated terms are then O(eps^2/d^2) instead of O(1),
+//    so FP32 accumulation error becomes negligible for far tiles.  Tiles near
+//    the target (sigma = 0) or straddling the image split use Kahan-compensated
+//    FP32 accumulation.  Every tile's partial sum is added into an FP64
+//    accumulator.
+//  * Per pair: FSUB, FFMA, MUFU.RSQ, FFMA, FFMA -- bound by the MUFU pipe
+//    (16 rsqrt/clk/SM), with source tiles moved global->shared by TMA bulk
+//    copies (cp.async.bulk, no multicast) double-buffered on mbarriers.
+//
+// Work is split over (target block, source chunk) CTAs; chunk partials are
+// summed in a fixed order by the finalize kernel, which also applies the fused
+// RK4 stage epilogue.
+#include <cub/cub.cuh>
+
+#include "fs_device.cuh"
+
+namespace fsb {
+
+namespace {
+
+constexpr int kS = 256;          // sources per tile
+constexpr int kNT = 128;         // threads per CTA
+constexpr int kR = 4;            // targets per thread
+constexpr int kTB = kNT * kR;    // targets per CTA
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// 1-D bulk copy global -> shared (TMA), completion signalled on `bar`.
+// Source and destination are 16-byte aligned and bytes is a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, "
+        "p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (long long it = 0; it < (1LL << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// One MUFU.RSQ: the argument is >= eps^2 > 0, never denormal.
+__device__ __forceinline__ float rsqrt_approx(float v) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+}
+
+__device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_double((long long)k); }
+
+// x -> [0, L) and its order-preserving key (non-negative doubles sort as
+// unsigned integers).
+__global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint64_t* __restrict__ keys,
+                            int* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double w = x[i] - L * floor(x[i] / L);
+    if (w >= L) w -= L;
+    if (w < 0.0) w = 0.0;
+    w = w + 0.0;  // -0 -> +0
+    keys[i] = (uint64_t)__double_as_longlong(w);
+    idx[i] = i;
+}
+
+// Sorted sources -> tile-relative FP32 records {s, q/2}; pads get {0, 0}.
+// Also the FP64 sorted q and q*x for the background sums.
+__global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
+                                 const double* __restrict__ q, int ns, int ns_pad, float2* __restrict__ src2,
+                                 double* __restrict__ qs, double* __restrict__ qx) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns_pad) return;
+    if (j >= ns) {
+        src2[j] = make_float2(0.f, 0.f);
+        return;
+    }
+    const double xj = key_to_x(skeys[j]);
+    const double base = key_to_x(skeys[(j / kS) * kS]);
+    const double qj = q[sidx[j]];
+    src2[j] = make_float2((float)(xj - base), (float)(0.5 * qj));
+    qs[j] = qj;
+    qx[j] = qj * xj;
+}
+
+// Per tile: FP64 base, largest FP32 offset, and the FP64 sum of the FP32 q/2
+// actually used by the pair kernel (one warp per tile, fixed reduction order).
+__global__ void k_tile_stats(const float2* __restrict__ src2, const uint64_t* __restrict__ skeys, int ns,
+                             int ntiles, double* __restrict__ tbase, float* __restrict__ tsmax,
+                             double* __restrict__ tqh) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ntiles) return;
+    const int j0 = warp * kS;
+    double s = 0.0;
+    for (int k = lane; k < kS; k += 32) s += (double)src2[j0 + k].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const int jl = min(ns - 1, j0 + kS - 1);
+        tbase[warp] = key_to_x(skeys[j0]);
+        tsmax[warp] = src2[jl].x;
+        tqh[warp] = s;
+    }
+}
+
+// Per sorted target: its image split J (first source index whose periodic
+// image differs) and the target coordinate used for sources before J.
+__global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt_pad,
+                              const uint64_t* __restrict__ skeys, int ns, double L, double* __restrict__ tlo,
+                              int* __restrict__ tJ) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt_pad) return;
+    if (i >= nt) {
+        tlo[i] = 0.0;
+        tJ[i] = 0;
+        return;
+    }
+    const double xw = key_to_x(tkeys[i]);
+    const double half = 0.5 * L;
+    double th, shift;
+    if (xw < half) {
+        th = xw + half;   // sources at or beyond x_i + L/2 use the image +L
+        shift = 0.0;
+    } else {
+        th = xw - half;   // sources below x_i - L/2 use the image -L
+        shift = -L;
+    }
+    int lo = 0, hi = ns;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (key_to_x(skeys[mid]) < th) lo = mid + 1;
+        else hi = mid;
+    }
+    tJ[i] = lo;
+    tlo[i] = xw + shift;
+}
+
+template <int R>
+struct TileSetup {
+    float tau[R], tauh[R], nsg[R], sg[R];
+};
+
+__global__ void __launch_bounds__(kNT)
+k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, const float* __restrict__ tsmax,
+          const double* __restrict__ tqh, int ntiles, int tiles_per_chunk, const double* __restrict__ tlo,
+          const int* __restrict__ tJ, int nt_pad, double L, float eps2, double* __restrict__ partial,
+          int* __restrict__ err) {
+    __shared__ __align__(128) float2 buf[2][kS];
+    __shared__ __align__(8) uint64_t bar[2];
+    const int tid = threadIdx.x;
+    const int t0 = blockIdx.y * tiles_per_chunk;
+    const int t1 = min(ntiles, t0 + tiles_per_chunk);
+    if (t0 >= t1) return;
+    const int ibase = blockIdx.x * kTB + tid;
+    double tl[kR], acc64[kR];
+    int J[kR];
+#pragma unroll
+    for (int r = 0; r < kR; ++r) {
+        const int i = ibase + r * kNT;  // nt_pad is a multiple of kTB: always in range
+        tl[r] = tlo[i];
+        J[r] = tJ[i];
+        acc64[r] = 0.0;
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    constexpr uint32_t kBytes = kS * sizeof(float2);
+    if (tid == 0) {
+        mbar_expect_tx(&bar[0], kBytes);
+        bulk_load(buf[0], src2 + (size_t)t0 * kS, kBytes, &bar[0]);
+    }
+    for (int t = t0; t < t1; ++t) {
+        const int k = t - t0;
+        const int b = k & 1;
+        if (tid == 0 && t + 1 < t1) {
+            fence_proxy_async();
+            mbar_expect_tx(&bar[b ^ 1], kBytes);
+            bulk_load(buf[b ^ 1], src2 + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
+        }
+        const bool ok = mbar_wait_bounded(&bar[b], (uint32_t)((k >> 1) & 1));
+        if (!__syncthreads_and(ok)) {
+            if (tid == 0) {
+                atomicExch(err, (int)FS_ERR_TIMEOUT);
+                // let a copy still in flight land before the CTA's shared memory is released
+                if (t + 1 < t1) (void)mbar_wait_bounded(&bar[b ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        const double base = tbase[t];
+        const float smax = tsmax[t];
+        const int jlo = t * kS;
+        float tau[kR], tauh[kR], nsg[kR], sg[kR], acc[kR];
+        bool careful = false;
+#pragma unroll
+        for (int r = 0; r < kR; ++r) {
+            const double lo = tl[r] - base;
+            const bool all_lo = (jlo + kS <= J[r]);
+            const bool all_hi = (jlo >= J[r]);
+            const float a = (float)(all_hi ? lo + L : lo);
+            tau[r] = a;
+            tauh[r] = (all_lo || all_hi) ? a : (float)(lo + L);
+            float s = 0.f;
+            if (all_lo || all_hi) s = (a > smax) ? 1.f : ((a < 0.f) ? -1.f : 0.f);
+            sg[r] = s;
+            nsg[r] = -s;
+            acc[r] = 0.f;
+            careful |= (s == 0.f);
+        }
+        const float2* tile = buf[b];
+        if (!__any_sync(0xffffffffu, careful)) {
+            // far tiles: every lane's tile lies on one side of its targets
+#pragma unroll 4
+            for (int j = 0; j < kS; ++j) {
+                const float2 e = tile[j];
+#pragma unroll
+                for (int r = 0; r < kR; ++r) {
+                    const float d = tau[r] - e.x;
+                    const float y = rsqrt_approx(fmaf(d, d, eps2));
+                    const float u = fmaf(d, y, nsg[r]);
+                    acc[r] = fmaf(e.y, u, acc[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kR; ++r) acc64[r] += (double)acc[r] + (double)sg[r] * tqh[t];
+        } else {
+            // near / image-split tiles: per-pair image, Kahan-compensated sum
+            float cmp[kR];
+#pragma unroll
+            for (int r = 0; r < kR; ++r) cmp[r] = 0.f;
+            for (int j = 0; j < kS; ++j) {
+                const float2 e = tile[j];
+                const int idx = jlo + j;
+#pragma unroll
+                for (int r = 0; r < kR; ++r) {
+                    const float tr = (idx < J[r]) ? tau[r] : tauh[r];
+                    const float d = tr - e.x;
+                    const float y = rsqrt_approx(fmaf(d, d, eps2));
+                    const float u = fmaf(d, y, nsg[r]);
+                    const float v = fmaf(e.y, u, -cmp[r]);
+                    const float s = acc[r] + v;
+                    cmp[r] = (s - acc[r]) - v;
+                    acc[r] = s;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kR; ++r)
+                acc64[r] += ((double)acc[r] - (double)cmp[r]) + (double)sg[r] * tqh[t];
+        }
+        __syncthreads();
+    }
+    double* out = partial + (size_t)blockIdx.y * nt_pad;
+#pragma unroll
+    for (int r = 0; r < kR; ++r) out[ibase + r * kNT] = acc64[r];
+}
+
+// Sum the chunk partials in a fixed order, subtract the FP64 background and
+// apply the stage epilogue at the target's original index.
+__global__ void k_finalize32(const double* __restrict__ partial, int nchunks, int nt_pad, int nt,
+                             const double* __restrict__ tlo, const int* __restrict__ tJ,
+                             const double* __restrict__ pq, const double* __restrict__ qxsum, int ns, double L,
+                             double cbg, const int* __restrict__ tperm, Stage S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt) return;
+    double E = 0.0;
+    for (int c = 0; c < nchunks; ++c) E += partial[(size_t)c * nt_pad + i];
+    if (ns > 0) {
+        const double Q = pq[ns - 1];
+        const int J = tJ[i];
+        const double PJ = (J > 0) ? pq[J - 1] : 0.0;
+        const double B = tlo[i] * Q - qxsum[0] + L * (Q - PJ);
+        E -= cbg * B;
+    }
+    apply_stage(S, tperm[i], E);
+}
+
+class Direct32c final : public FieldEngine {
+   public:
+    Direct32c(double L, double eps) : L_(L), eps_(eps) { cbg_ = 1 / std::sqrt(L * L + 4 * eps * eps); }
+
+    void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
+              cudaStream_t st) override {
+        last_pairs = (double)nt * (double)ns;
+        if (nt <= 0) return;
+        const bool same = (d_t == d_s) && (nt == ns);
+        const int ntiles = (ns + kS - 1) / kS;
+        const int ns_pad = ntiles * kS;
+        const int tblocks = (nt + kTB - 1) / kTB;
+        const int nt_pad = tblocks * kTB;
+        const int sms = sm_count();
+        // enough CTAs for several waves at ~8 resident CTAs per SM
+        const int want = sms * 8 * 4;
+        int nchunks = ntiles ? std::min(ntiles, std::max(1, (want + tblocks - 1) / tblocks)) : 1;
+        const int tpc = ntiles ? (ntiles + nchunks - 1) / nchunks : 1;
+        nchunks = ntiles ? (ntiles + tpc - 1) / tpc : 1;
+        reserve(std::max(ns, 1), ns_pad, same ? 0 : nt, nt_pad, (size_t)nchunks * nt_pad, ntiles);
+        const int T = 256;
+        const uint64_t* tkeys;
+        const int* tperm;
+        if (ns > 0) {
+            k_wrap_keys<<<(ns + T - 1) / T, T, 0, st>>>(d_s, ns, L_, kin_.p, iin_.p);
+            size_t tb = cub_.bytes();
+            FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
+            k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, src2_.p, qs_.p,
+                                                                 qx_.p);
+            k_tile_stats<<<(ntiles * 32 + T - 1) / T, T, 0, st>>>(src2_.p, kout_.p, ns, ntiles, tbase_.p, tsmax_.p,
+                                                                  tqh_.p);
+            tb = cub_.bytes();
+            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
+            tb = cub_.bytes();
+            FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
+            FS_LAUNCHED(3);  // own kernels (the sort / scan / reduce kernels are CUB's)
+        }
+        if (same) {
+            tkeys = kout_.p;
+            tperm = iout_.p;
+        } else {
+            k_wrap_keys<<<(nt + T - 1) / T, T, 0, st>>>(d_t, nt, L_, tkin_.p, tiin_.p);
+            size_t tb = cub_.bytes();
+            FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, tkin_.p, tkout_.p, tiin_.p, tiout_.p, nt, 0, 63, st));
+            tkeys = tkout_.p;
+            tperm = tiout_.p;
+            FS_LAUNCHED(1);
+        }
+        if (ns > 0) {
+            k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, tlo_.p, tJ_.p);
+            dim3 grid(tblocks, nchunks);
+            ProfScope prof("k_pairs32", st, last_pairs);
+            k_pairs32<<<grid, kNT, 0, st>>>(src2_.p, tbase_.p, tsmax_.p, tqh_.p, ntiles, tpc, tlo_.p, tJ_.p, nt_pad,
+                                             L_, (float)(eps_ * eps_), partial_.p, err_.p);
+            FS_LAUNCHED(2);
+        } else {
+            FS_CUDA(cudaMemsetAsync(partial_.p, 0, sizeof(double) * nt_pad, st));
+            nchunks = 1;
+        }
+        k_finalize32<<<(nt + T - 1) / T, T, 0, st>>>(partial_.p, nchunks, nt_pad, nt, tlo_.p, tJ_.p, pq_.p,
+                                                      qxsum_.p, ns, L_, cbg_, tperm, stage);
+        FS_LAUNCHED(1);
+    }
+
+    int* error_flag() override { return err_.p; }
+
+   private:
+    void reserve(int ns, int ns_pad, int nt_sep, int nt_pad, size_t npartial, int ntiles) {
+        kin_.ensure(ns);
+        kout_.ensure(ns);
+        iin_.ensure(ns);
+        iout_.ensure(ns);
+        src2_.ensure(ns_pad);
+        qs_.ensure(ns);
+        qx_.ensure(ns);
+        pq_.ensure(ns);
+        qxsum_.ensure(1);
+        tbase_.ensure(std::max(ntiles, 1));
+        tsmax_.ensure(std::max(ntiles, 1));
+        tqh_.ensure(std::max(ntiles, 1));
+        tlo_.ensure(nt_pad);
+        tJ_.ensure(nt_pad);
+        partial_.ensure(npartial);
+        if (!err_.p) {
+            err_.ensure(1);
+            FS_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+        }
+        const int nsort = std::max(ns, nt_sep);
+        if (nt_sep) {
+            tkin_.ensure(nt_sep);
+            tkout_.ensure(nt_sep);
+            tiin_.ensure(nt_sep);
+            tiout_.ensure(nt_sep);
+        }
+        size_t need = 0, b = 0;
+        FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (int*)nullptr,
+                                                (int*)nullptr, nsort, 0, 63));
+        need = std::max(need, b);
+        FS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, (double*)nullptr, (double*)nullptr, ns));
+        need = std::max(need, b);
+        FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, (double*)nullptr, (double*)nullptr, ns));
+        need = std::max(need, b);
+        cub_.ensure(need);
+    }
+
+    double L_, eps_, cbg_;
+    DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
+    DevBuf<int> iin_, iout_, tiin_, tiout_;
+    DevBuf<float2> src2_;
+    DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, tqh_, tlo_, partial_;
+    DevBuf<float> tsmax_;
+    DevBuf<int> tJ_, err_;
+    DevBuf<unsigned char> cub_;
+};
+
+}  // namespace
+
+FieldEngine* make_direct32c(double L, double eps) { return new Direct32c(L, eps); }
+
+}  // namespace fsb

@@ -1,0 +1,153 @@
+// Internal declarations of libfs_b200 (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdint>
+#include <functional>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fs_b200.h"
+
+namespace fsb {
+
+// ------------------------------------------------------------------ errors
+// Internal code throws FsError; the C ABI layer converts it to an fs_status
+// and records the message for fs_last_error().
+struct FsError {
+    fs_status code;
+    std::string msg;
+};
+
+void set_last_error(const std::string& msg);
+[[noreturn]] void fail(fs_status code, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+
+#define FS_CUDA(call) ::fsb::cuda_check((call), #call, __FILE__, __LINE__)
+#define FS_LAUNCHED(n) do { ::fsb::count_launches(n); FS_CUDA(cudaGetLastError()); } while (0)
+
+void count_launches(long long n);
+long long launches();
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Device-time profiling of named kernels (enabled by fs_profile_enable).
+// Records a CUDA event pair on `st` around the enclosed launches.
+class ProfScope {
+   public:
+    // `work`: algorithmic units done by the enclosed launches (pairs, bytes)
+    ProfScope(const char* name, cudaStream_t st, double work = 0.0);
+    ~ProfScope();
+    ProfScope(const ProfScope&) = delete;
+    ProfScope& operator=(const ProfScope&) = delete;
+
+   private:
+    const char* name_;
+    cudaStream_t st_;
+    double work_;
+    cudaEvent_t a_ = nullptr, b_ = nullptr;
+};
+bool profiling_enabled();
+
+// ------------------------------------------------------------------ device buffers
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t bytes = (count ? count : 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            (void)cudaGetLastError();
+            fail(FS_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------ RK4 stage epilogue
+// Fused into the last kernel of each field evaluation.  kind:
+//   STAGE_STORE  out[o] = E
+//   STAGE_RK2    E is the field at the stage-2 positions: ef2 = E*qm,
+//                p3 = p + hdt*ef2, xk = x + hdt*p2, accX += 2 p2, accP += 2 ef2
+//   STAGE_RK3    ef3 = E*qm, p4 = p + dt*ef3, xk = x + dt*p3, accX += 2 p3, accP += 2 ef3
+//   STAGE_RK4    ef4 = E*qm, x += dt6*(accX + p4), p += dt6*(accP + ef4)
+// (src/simulation_files/AMRSimulation_step.cpp:158-248, same operation order).
+enum StageKind { STAGE_STORE = 0, STAGE_RK2 = 1, STAGE_RK3 = 2, STAGE_RK4 = 3 };
+
+struct Stage {
+    int kind = STAGE_STORE;
+    double* out = nullptr;
+    double *x = nullptr, *p = nullptr, *xk = nullptr, *pst = nullptr, *accX = nullptr, *accP = nullptr;
+    double dt = 0, hdt = 0, dt6 = 0;
+    int nsp = 1;
+    int start[9] = {0};
+    double qm[8] = {0};
+};
+
+// ------------------------------------------------------------------ host mesh
+struct HostPanel {
+    int pts[9];
+    int level, parent, which, child;
+    int left, top, right, bottom;
+    uint8_t lb, rb, xp, pr, needs;
+};
+
+struct HostMesh {
+    int h = 0, ph = 0;
+    double xmin = 0, xmax = 0, pmin = 0, pmax = 0;
+    std::vector<HostPanel> panels;
+    std::vector<double> xs, ps;
+    std::vector<int> leaves;
+    void build(int h, int ph, double xmin, double xmax, double pmin, double pmax);
+    std::vector<double> base_weights(double q, int quadrature) const;
+    void panel_records(int* out) const;  // 18 ints per panel
+    int nx() const { return 2 * (1 << h) + 1; }
+    int np() const { return 2 * (1 << (h + ph)) + 1; }
+};
+
+double f0_value(int ics_type, double pth, double pstr, double k, double amp, double x, double p);
+
+// ------------------------------------------------------------------ field engines
+class FieldEngine {
+   public:
+    virtual ~FieldEngine() = default;
+    // Field at targets from sources (device pointers), result through the
+    // stage epilogue, enqueued on `st`.  For targets == sources pass the same
+    // pointer and nt == ns.
+    virtual void eval(const double* d_targets, int nt, const double* d_sources, const double* d_q,
+                      int ns, const Stage& stage, cudaStream_t st) = 0;
+    // Device int set non-zero by a kernel whose bounded wait gave up (or null).
+    virtual int* error_flag() { return nullptr; }
+    // Pair interactions (direct-equivalent) of the last call.
+    double last_pairs = 0;
+};
+
+// Runs fn, converting FsError / exceptions into an fs_status and recording the
+// message for fs_last_error().
+fs_status guard(const std::function<void()>& fn);
+
+FieldEngine* make_direct64(double L, double eps);
+FieldEngine* make_direct32c(double L, double eps);
+FieldEngine* make_treecode(double L, double eps, double mac, int degree, int max_source, bool fp32_near);
+
+}  // namespace fsb

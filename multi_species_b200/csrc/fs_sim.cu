@@ -1,0 +1,689 @@
+// Device-resident FARRSIGHT simulation: RK4 step, remesh, reduced-grid field.
+//
+// Host control flow follows AMRSimulation::step (src/simulation_files/AMRSimulation_step.cpp:5-99):
+//   RK4 (3 field evaluations at stage positions, epilogues fused into the field
+//   kernels) -> iter++, t += dt -> remesh + reduced-grid field every
+//   remesh_period steps, otherwise a 4th field evaluation at the new positions.
+// All species live in one concatenated SoA (x, p, f, q_w, E) in HBM, species
+// ranges contiguous, so AMRSimulation::gather/scatter
+// (AMRSimulation_gather_scatter.cpp:3-51) are index ranges, not copies.
+//
+// Remesh per species (AMRStructure::remesh, AMRStructure_amr.cpp:1156-1202):
+//   k_panel_fit    one thread per old leaf: 9x9 LU fit of f about point 4
+//                  (interpolate_from_panel_to_points, AMRStructure_interp.cpp:795-975)
+//   k_locate_eval  one thread per new lattice point: periodic shift into the
+//                  sheared root (shift_xs :429-491), start at the panel the
+//                  point's material came from, then the reference's neighbour
+//                  walk (find_leaf_containing_point_from_neighbor :12-230) with
+//                  its half-open edge tests, bounded; evaluate the fit or
+//                  f_beyond_boundary.
+//   k_reset_points x,p <- lattice, f <- new f, q_w <- w0 * f
+//                  (set_leaves_weights :1084-1151 with cached w0).
+// Reduced grid (evaluate_field_uniform_grid, AMRSimulation_field.cpp:5-162,
+// get_reduced_xs_ws AMRStructure.cpp:147-196): the lattice's unique x and the
+// point->unique map are fixed, so they are cached; per remesh only the
+// per-column charge sums (in the reference's summation order) are formed.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <memory>
+
+#include "fs_device.cuh"
+
+namespace fsb {
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kWalkLimit = 4096;
+constexpr int kHist = 32;
+
+__device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
+
+// ---------------------------------------------------------------- RK4 stage 1
+// ef1 = E*qm, p2 = p + hdt*ef1, xk = x + hdt*p, accX = p, accP = ef1
+// (AMRSimulation_step.cpp:148-165).
+__global__ void k_rk_stage1(int n, Stage S, double* __restrict__ e, double* __restrict__ xk) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    const double ef = dmul(e[o], stage_qm(S, o));
+    const double p1 = S.p[o];
+    S.pst[o] = dadd(p1, dmul(S.hdt, ef));
+    xk[o] = dadd(S.x[o], dmul(S.hdt, p1));
+    S.accX[o] = p1;
+    S.accP[o] = ef;
+}
+
+// ---------------------------------------------------------------- 9-point fit
+// Row pivoting by the largest |a| (first on ties); the algorithm class of the
+// reference's Eigen PartialPivLU (AMRStructure_interp.cpp:935).
+__device__ void lu_solve9(double A[9][9], double b[9]) {
+    int perm[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) perm[i] = i;
+    for (int k = 0; k < 9; ++k) {
+        int piv = k;
+        double best = fabs(A[k][k]);
+        for (int i = k + 1; i < 9; ++i) {
+            const double v = fabs(A[i][k]);
+            if (v > best) {
+                best = v;
+                piv = i;
+            }
+        }
+        if (piv != k) {
+            for (int j = 0; j < 9; ++j) {
+                const double t = A[k][j];
+                A[k][j] = A[piv][j];
+                A[piv][j] = t;
+            }
+            const int t = perm[k];
+            perm[k] = perm[piv];
+            perm[piv] = t;
+        }
+        if (best != 0.0)
+            for (int i = k + 1; i < 9; ++i) A[i][k] = ddiv(A[i][k], A[k][k]);
+        for (int i = k + 1; i < 9; ++i)
+            for (int j = k + 1; j < 9; ++j) A[i][j] = dsub(A[i][j], dmul(A[i][k], A[k][j]));
+    }
+    double y[9];
+    for (int i = 0; i < 9; ++i) y[i] = b[perm[i]];
+    for (int k = 0; k < 9; ++k)
+        for (int i = k + 1; i < 9; ++i) y[i] = dsub(y[i], dmul(y[k], A[i][k]));
+    for (int k = 8; k >= 0; --k) {
+        y[k] = ddiv(y[k], A[k][k]);
+        for (int i = 0; i < k; ++i) y[i] = dsub(y[i], dmul(y[k], A[i][k]));
+    }
+    for (int i = 0; i < 9; ++i) b[i] = y[i];
+}
+
+// coef[slot*11 + 0..8] = c, [9] = x4, [10] = p4
+__global__ void k_panel_fit(int nleaves, const int* __restrict__ leaves, const int* __restrict__ rec,
+                            const double* __restrict__ ox, const double* __restrict__ op,
+                            const double* __restrict__ of, double* __restrict__ coef) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nleaves) return;
+    const int* r = rec + (size_t)leaves[l] * 18;
+    double px[9], pp[9], A[9][9], c[9];
+    for (int i = 0; i < 9; ++i) {
+        px[i] = ox[r[i]];
+        pp[i] = op[r[i]];
+        c[i] = of[r[i]];
+    }
+    for (int i = 0; i < 9; ++i) {
+        const double dx = dsub(px[i], px[4]), dp = dsub(pp[i], pp[4]);
+        A[i][0] = 1;
+        A[i][1] = dx;
+        A[i][2] = dmul(dx, dp);
+        A[i][3] = dp;
+        A[i][4] = dmul(dx, dx);
+        A[i][5] = dmul(dmul(dx, dx), dp);
+        A[i][6] = dmul(dmul(dmul(dx, dx), dp), dp);
+        A[i][7] = dmul(dmul(dx, dp), dp);
+        A[i][8] = dmul(dp, dp);
+    }
+    lu_solve9(A, c);
+    double* o = coef + (size_t)l * 11;
+    for (int i = 0; i < 9; ++i) o[i] = c[i];
+    o[9] = px[4];
+    o[10] = pp[4];
+}
+
+struct MeshView {
+    const int* rec;        // 18 ints per panel
+    const int* leaf_slot;  // panel -> leaf slot (or -1)
+    const int* cell_leaf;  // (ix * npp + ip) -> leaf panel of the lattice cell
+    const double* lat_x;
+    const double* lat_p;
+    const double* coef;
+    int npx, npp, n;
+    double xmin, pmin, Lx, dxp, dpp;
+    double f_beyond;
+    double shear_t;        // time since the mesh was last reset (start guess)
+};
+
+__device__ __forceinline__ bool edge_right(double x_tr, double p_tr, double x_br, double p_br, double tx, double tp) {
+    return dmul(dsub(x_tr, x_br), dsub(tp, p_br)) > dmul(dsub(p_tr, p_br), dsub(tx, x_br));
+}
+__device__ __forceinline__ bool edge_left(double x_tl, double p_tl, double x_bl, double p_bl, double tx, double tp) {
+    return dmul(dsub(x_tl, x_bl), dsub(tp, p_bl)) <= dmul(dsub(p_tl, p_bl), dsub(tx, x_bl));
+}
+__device__ __forceinline__ bool edge_top(double x_tr, double p_tr, double x_tl, double p_tl, double tx, double tp) {
+    return dmul(dsub(x_tr, x_tl), dsub(tp, p_tl)) < dmul(dsub(p_tr, p_tl), dsub(tx, x_tl));
+}
+__device__ __forceinline__ bool edge_bottom(double x_br, double p_br, double x_bl, double p_bl, double tx, double tp) {
+    return dmul(dsub(x_br, x_bl), dsub(tp, p_bl)) >= dmul(dsub(p_br, p_bl), dsub(tx, x_bl));
+}
+
+__global__ void k_locate_eval(MeshView M, const double* __restrict__ ox, const double* __restrict__ op,
+                              double* __restrict__ fnew, int* __restrict__ status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M.n) return;
+    const double tp = M.lat_p[k];
+    double tx = M.lat_x[k];
+    const double Lx = M.Lx;
+    // shift_xs: into the sheared root panel (old points 0, 2, 6, 8)
+    {
+        const double x_bl = ox[0], p_bl = op[0], x_tl = ox[2], p_tl = op[2];
+        const double x_br = ox[6], p_br = op[6], x_tr = ox[8], p_tr = op[8];
+        int cnt = 0;
+        while (!edge_left(x_tl, p_tl, x_bl, p_bl, tx, tp)) {
+            tx = dadd(tx, Lx);
+            if (++cnt > 10) {
+                raise_status(status, FS_ERR_SHIFT);
+                return;
+            }
+        }
+        cnt = 0;
+        while (!edge_right(x_tr, p_tr, x_br, p_br, tx, tp)) {
+            tx = dsub(tx, Lx);
+            if (++cnt > 10) {
+                raise_status(status, FS_ERR_SHIFT);
+                return;
+            }
+        }
+    }
+    // start at the panel whose material streamed to this point
+    double xg = tx - tp * M.shear_t - M.xmin;
+    xg -= Lx * floor(xg / Lx);
+    int ix = (int)floor(xg / M.dxp);
+    ix = min(max(ix, 0), M.npx - 1);
+    int ip = (int)floor((tp - M.pmin) / M.dpp);
+    ip = min(max(ip, 0), M.npp - 1);
+    int leaf = M.cell_leaf[ix * M.npp + ip];
+    int hist[kHist];
+    int nh = 0;
+    hist[nh++] = leaf;
+    bool beyond = false;
+    int steps = 0;
+    const int* R = M.rec;
+    for (;;) {
+        if (leaf == 0) break;
+        const int* P = R + (size_t)leaf * 18;
+        const double x_bl = ox[P[0]], p_bl = op[P[0]];
+        const double x_tl = ox[P[2]], p_tl = op[P[2]];
+        const double x_mid = ox[P[4]];
+        const double x_br = ox[P[6]], p_br = op[P[6]];
+        const double x_tr = ox[P[8]], p_tr = op[P[8]];
+        if (dsub(tx, x_mid) >= Lx / 2) tx = dsub(tx, Lx);
+        if (dsub(tx, x_mid) < -Lx / 2) tx = dadd(tx, Lx);
+        const bool ir = edge_right(x_tr, p_tr, x_br, p_br, tx, tp);
+        const bool il = edge_left(x_tl, p_tl, x_bl, p_bl, tx, tp);
+        const bool it = edge_top(x_tr, p_tr, x_tl, p_tl, tx, tp);
+        const bool ib = edge_bottom(x_br, p_br, x_bl, p_bl, tx, tp);
+        const int left = P[13], top = P[14], right = P[15], bottom = P[16], flags = P[17], parent = P[10];
+        int nl = leaf;
+        if (!ir && right != -2) {
+            if (flags & 2) tx = dsub(tx, Lx);
+            if (right == -1) nl = R[(size_t)parent * 18 + 15];
+            else nl = (R[(size_t)right * 18 + 17] & 4) ? R[(size_t)right * 18 + 12] : right;
+        } else if (!it && top != -2) {
+            if (top == -1) nl = R[(size_t)parent * 18 + 14];
+            else nl = (R[(size_t)top * 18 + 17] & 4) ? R[(size_t)top * 18 + 12] : top;
+        } else if (!ib && bottom != -2) {
+            if (bottom == -1) nl = R[(size_t)parent * 18 + 16];
+            else nl = (R[(size_t)bottom * 18 + 17] & 4) ? R[(size_t)bottom * 18 + 12] + 1 : bottom;
+        } else if (!il && left != -2) {
+            if (flags & 1) tx = dadd(tx, Lx);
+            if (left == -1) nl = R[(size_t)parent * 18 + 13];
+            else nl = (R[(size_t)left * 18 + 17] & 4) ? R[(size_t)left * 18 + 12] + 2 : left;
+        }
+        if ((!ir && right == -2) || (!il && left == -2) || (!it && top == -2) || (!ib && bottom == -2))
+            beyond = true;
+        bool seen = false;
+        for (int h = 0; h < min(nh, kHist); ++h) seen |= (hist[h] == nl);
+        leaf = nl;
+        if (seen) break;
+        hist[nh % kHist] = nl;
+        ++nh;
+        if (++steps > kWalkLimit) {
+            raise_status(status, FS_ERR_WALK);
+            return;
+        }
+    }
+    double v;
+    const int slot = (leaf > 0) ? M.leaf_slot[leaf] : -1;
+    if (beyond || leaf == 0 || slot < 0) {
+        v = M.f_beyond;
+    } else {
+        const double* c = M.coef + (size_t)slot * 11;
+        const double dx = dsub(tx, c[9]), dp = dsub(tp, c[10]);
+        const double dxsq = dmul(dx, dx), dpsq = dmul(dp, dp);
+        const double D[9] = {1.0, dx, dmul(dx, dp), dp, dxsq, dmul(dxsq, dp), dmul(dxsq, dpsq), dmul(dx, dpsq), dpsq};
+        v = 0.0;
+        for (int j = 0; j < 9; ++j) v = dadd(v, dmul(D[j], c[j]));
+    }
+    fnew[k] = v;
+}
+
+__global__ void k_reset_points(int n, const double* __restrict__ lat_x, const double* __restrict__ lat_p,
+                               const double* __restrict__ w0, const double* __restrict__ fnew, double* __restrict__ x,
+                               double* __restrict__ p, double* __restrict__ f, double* __restrict__ qw) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    x[k] = lat_x[k];
+    p[k] = lat_p[k];
+    f[k] = fnew[k];
+    qw[k] = dmul(w0[k], fnew[k]);
+}
+
+// reduced_ws[u] = sum of q_w over the points of unique x u, in point order
+__global__ void k_column_sums(int nu, const int* __restrict__ off, const int* __restrict__ idx,
+                              const double* __restrict__ qw, double* __restrict__ rw) {
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= nu) return;
+    double s = 0.0;
+    for (int k = off[u]; k < off[u + 1]; ++k) s = dadd(s, qw[idx[k]]);
+    rw[u] = s;
+}
+
+__global__ void k_scatter_reduced(int n, const int* __restrict__ inv, const double* __restrict__ re,
+                                  double* __restrict__ e) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    e[k] = re[inv[k]];
+}
+
+template <class T>
+void upload(DevBuf<T>& b, const std::vector<T>& h) {
+    b.ensure(h.size());
+    if (!h.empty()) FS_CUDA(cudaMemcpy(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+}
+
+inline int blocks(int n) { return (n + kT - 1) / kT; }
+
+}  // namespace
+
+struct SpeciesState {
+    HostMesh mesh;
+    int start = 0, n = 0;
+    double q = 0, m = 0, qm = 0, f_beyond = 0;
+    int nleaves = 0, npx = 0, npp = 0;
+    DevBuf<double> lat_x, lat_p, w0, coef, fnew;
+    DevBuf<int> rec, leaf_slot, leaves, cell_leaf;
+    // reduced grid
+    int nu = 0, roff = 0;
+    DevBuf<int> inv, col_off, col_idx;
+};
+
+struct Sim {
+    fs_sim_params prm{};
+    int N = 0, U = 0, iter = 0;
+    double L = 0, t = 0, t_reset = 0, pairs = 0;
+    std::vector<std::unique_ptr<SpeciesState>> sp;
+    DevBuf<double> x, p, f, qw, e, xkA, xkB, pst, accX, accP, rx, rw, re;
+    DevBuf<int> status;
+    std::unique_ptr<FieldEngine> field;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<double> step_ms;
+    Stage base;
+
+    ~Sim() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    void check_status() {
+        FS_CUDA(cudaStreamSynchronize(st));
+        int h = 0;
+        FS_CUDA(cudaMemcpy(&h, status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h == 0 && field) {
+            if (int* fe = field_error_flag(field.get())) {
+                FS_CUDA(cudaMemcpy(&h, fe, sizeof(int), cudaMemcpyDeviceToHost));
+                if (h) FS_CUDA(cudaMemset(fe, 0, sizeof(int)));
+            }
+        }
+        if (h) {
+            FS_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+            fail((fs_status)h, h == FS_ERR_WALK    ? "remesh point location did not converge"
+                               : h == FS_ERR_SHIFT ? "remesh: too many periodic shifts"
+                                                   : "device wait timed out");
+        }
+    }
+
+    void create(const fs_sim_params& P) {
+        prm = P;
+        if (P.num_species < 1 || P.num_species > 8) fail(FS_ERR_ARG, "num_species must be 1..8");
+        if (!(P.xmax > P.xmin)) fail(FS_ERR_ARG, "xmax must exceed xmin");
+        if (P.remesh_period < 1) fail(FS_ERR_ARG, "remesh_period must be >= 1");
+        FS_CUDA(cudaSetDevice(P.device));
+        FS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        FS_CUDA(cudaEventCreate(&ev0));
+        FS_CUDA(cudaEventCreate(&ev1));
+        L = P.xmax - P.xmin;
+        std::vector<double> hx, hp, hf, hqw;
+        std::vector<double> hrx;
+        base.nsp = P.num_species;
+        for (int s = 0; s < P.num_species; ++s) {
+            const fs_species_params& S = P.species[s];
+            auto ss = std::make_unique<SpeciesState>();
+            ss->mesh.build(S.initial_height, S.p_height, P.xmin, P.xmax, S.pmin, S.pmax);
+            HostMesh& M = ss->mesh;
+            ss->start = N;
+            ss->n = (int)M.xs.size();
+            ss->q = S.q;
+            ss->m = S.m;
+            ss->qm = S.q / S.m;
+            ss->npx = 1 << S.initial_height;
+            ss->npp = 1 << (S.initial_height + S.p_height);
+            ss->nleaves = (int)M.leaves.size();
+            base.start[s] = N;
+            base.qm[s] = ss->qm;
+            N += ss->n;
+            // initial condition and weights (AMRStructure ctor / generate_mesh / set_leaves_weights)
+            const double kx = 2.0 * M_PI / L * S.normalized_wavenumber;
+            std::vector<double> w0 = M.base_weights(S.q, P.quadrature);
+            double fmin = 0;
+            for (int i = 0; i < ss->n; ++i) {
+                const double fv = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, M.xs[i], M.ps[i]);
+                hx.push_back(M.xs[i]);
+                hp.push_back(M.ps[i]);
+                hf.push_back(fv);
+                hqw.push_back(w0[i] * fv);
+                if (i == 0 || fv < fmin) fmin = fv;
+            }
+            ss->f_beyond = fmin;
+            upload(ss->lat_x, M.xs);
+            upload(ss->lat_p, M.ps);
+            upload(ss->w0, w0);
+            std::vector<int> rec(M.panels.size() * 18);
+            M.panel_records(rec.data());
+            upload(ss->rec, rec);
+            upload(ss->leaves, M.leaves);
+            std::vector<int> slot(M.panels.size(), -1);
+            for (size_t l = 0; l < M.leaves.size(); ++l) slot[M.leaves[l]] = (int)l;
+            upload(ss->leaf_slot, slot);
+            // lattice cell -> leaf panel, from each leaf's lower-left corner
+            std::vector<int> cell((size_t)ss->npx * ss->npp, 0);
+            const double dxp = L / ss->npx, dpp = (S.pmax - S.pmin) / ss->npp;
+            for (int l : M.leaves) {
+                const int c0 = M.panels[l].pts[0];
+                int ix = (int)std::lround((M.xs[c0] - P.xmin) / dxp);
+                int ip = (int)std::lround((M.ps[c0] - S.pmin) / dpp);
+                ix = std::min(std::max(ix, 0), ss->npx - 1);
+                ip = std::min(std::max(ip, 0), ss->npp - 1);
+                cell[(size_t)ix * ss->npp + ip] = l;
+            }
+            upload(ss->cell_leaf, cell);
+            ss->coef.ensure((size_t)ss->nleaves * 11);
+            ss->fnew.ensure(ss->n);
+            // reduced grid of the lattice: unique x (strictly increasing, as
+            // get_reduced_xs_ws), point -> unique map, per-unique point lists
+            std::vector<int> order(ss->n);
+            for (int i = 0; i < ss->n; ++i) order[i] = i;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return M.xs[a] < M.xs[b]; });
+            std::vector<int> inv(ss->n);
+            std::vector<double> ux;
+            double val = M.xs[order[0]];
+            ux.push_back(val);
+            inv[order[0]] = 0;
+            for (int k = 1; k < ss->n; ++k) {
+                const double v = M.xs[order[k]];
+                if (v > val) {
+                    val = v;
+                    ux.push_back(v);
+                }
+                inv[order[k]] = (int)ux.size() - 1;
+            }
+            ss->nu = (int)ux.size();
+            ss->roff = U;
+            U += ss->nu;
+            std::vector<int> off(ss->nu + 1, 0), idx(ss->n);
+            for (int i = 0; i < ss->n; ++i) off[inv[i] + 1]++;
+            for (int u = 0; u < ss->nu; ++u) off[u + 1] += off[u];
+            std::vector<int> fill(off.begin(), off.end() - 1);
+            for (int i = 0; i < ss->n; ++i) idx[fill[inv[i]]++] = i;  // ascending point index per column
+            std::vector<int> inv_global(ss->n);
+            for (int i = 0; i < ss->n; ++i) inv_global[i] = inv[i] + ss->roff;
+            upload(ss->inv, inv_global);
+            upload(ss->col_off, off);
+            upload(ss->col_idx, idx);
+            hrx.insert(hrx.end(), ux.begin(), ux.end());
+            sp.push_back(std::move(ss));
+        }
+        base.start[P.num_species] = N;
+        for (int s = P.num_species + 1; s < 9; ++s) base.start[s] = N;
+        base.dt = P.dt;
+        base.hdt = 0.5 * P.dt;
+        base.dt6 = P.dt / 6.0;
+        upload(x, hx);
+        upload(p, hp);
+        upload(f, hf);
+        upload(qw, hqw);
+        e.ensure(N);
+        xkA.ensure(N);
+        xkB.ensure(N);
+        pst.ensure(N);
+        accX.ensure(N);
+        accP.ensure(N);
+        upload(rx, hrx);
+        rw.ensure(U);
+        re.ensure(U);
+        status.ensure(1);
+        FS_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+        switch (P.field_kind) {
+            case FS_FIELD_DIRECT64: field.reset(make_direct64(L, P.greens_epsilon)); break;
+            case FS_FIELD_DIRECT32C: field.reset(make_direct32c(L, P.greens_epsilon)); break;
+            case FS_FIELD_TREECODE64:
+            case FS_FIELD_TREECODE32C:
+                field.reset(make_treecode(L, P.greens_epsilon, P.mac, P.degree, P.max_source,
+                                          P.field_kind == FS_FIELD_TREECODE32C));
+                break;
+            default: fail(FS_ERR_ARG, "unknown field kind");
+        }
+        base.x = x.p;
+        base.p = p.p;
+        base.pst = pst.p;
+        base.accX = accX.p;
+        base.accP = accP.p;
+        reduced_field();  // AMRSimulation ctor: evaluate_field_uniform_grid(0)
+        check_status();
+    }
+
+    Stage stage(int kind, double* xk_out) const {
+        Stage S = base;
+        S.kind = kind;
+        S.xk = xk_out;
+        return S;
+    }
+
+    void reduced_field() {
+        for (auto& s : sp) {
+            k_column_sums<<<blocks(s->nu), kT, 0, st>>>(s->nu, s->col_off.p, s->col_idx.p, qw.p + s->start,
+                                                       rw.p + s->roff);
+        }
+        FS_LAUNCHED((long long)sp.size());
+        Stage S = base;
+        S.kind = STAGE_STORE;
+        S.out = re.p;
+        field->eval(rx.p, U, rx.p, rw.p, U, S, st);
+        pairs += field->last_pairs;
+        for (auto& s : sp) {
+            k_scatter_reduced<<<blocks(s->n), kT, 0, st>>>(s->n, s->inv.p, re.p, e.p + s->start);
+        }
+        FS_LAUNCHED((long long)sp.size());
+    }
+
+    void remesh() {
+        for (auto& s : sp) {
+            const int a = s->start;
+            ProfScope prof("remesh", st);
+            k_panel_fit<<<blocks(s->nleaves), 128, 0, st>>>(s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a,
+                                                            f.p + a, s->coef.p);
+            MeshView M;
+            M.rec = s->rec.p;
+            M.leaf_slot = s->leaf_slot.p;
+            M.cell_leaf = s->cell_leaf.p;
+            M.lat_x = s->lat_x.p;
+            M.lat_p = s->lat_p.p;
+            M.coef = s->coef.p;
+            M.npx = s->npx;
+            M.npp = s->npp;
+            M.n = s->n;
+            M.xmin = prm.xmin;
+            M.pmin = s->mesh.pmin;
+            M.Lx = L;
+            M.dxp = L / s->npx;
+            M.dpp = (s->mesh.pmax - s->mesh.pmin) / s->npp;
+            M.f_beyond = s->f_beyond;
+            M.shear_t = t - t_reset;
+            k_locate_eval<<<blocks(s->n), 128, 0, st>>>(M, x.p + a, p.p + a, s->fnew.p, status.p);
+            k_reset_points<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
+                                                       p.p + a, f.p + a, qw.p + a);
+        }
+        FS_LAUNCHED(3LL * (long long)sp.size());
+        t_reset = t;
+        reduced_field();
+    }
+
+    void step() {
+        // RK4 (AMRSimulation_step.cpp:122-263); stage positions alternate
+        // between two buffers so no kernel writes the positions it reads.
+        Stage S1 = base;
+        k_rk_stage1<<<blocks(N), kT, 0, st>>>(N, S1, e.p, xkA.p);
+        FS_LAUNCHED(1);
+        field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK2, xkB.p), st);
+        pairs += field->last_pairs;
+        field->eval(xkB.p, N, xkB.p, qw.p, N, stage(STAGE_RK3, xkA.p), st);
+        pairs += field->last_pairs;
+        field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK4, nullptr), st);
+        pairs += field->last_pairs;
+        iter += 1;
+        t += prm.dt;
+        if (iter % prm.remesh_period == 0) {
+            remesh();
+        } else {
+            Stage S = base;
+            S.kind = STAGE_STORE;
+            S.out = e.p;
+            field->eval(x.p, N, x.p, qw.p, N, S, st);
+            pairs += field->last_pairs;
+        }
+    }
+
+    static int* field_error_flag(FieldEngine* fe) { return fe->error_flag(); }
+};
+
+}  // namespace fsb
+
+// ------------------------------------------------------------------ C ABI (session)
+struct fs_sim {
+    fsb::Sim impl;
+};
+
+extern "C" {
+
+fs_status fs_sim_create(const fs_sim_params* params, fs_sim** out) {
+    if (!params || !out) return fsb::guard([] { fsb::fail(FS_ERR_ARG, "null argument"); });
+    *out = nullptr;
+    auto* s = new fs_sim();
+    fs_status rc = fsb::guard([&] { s->impl.create(*params); });
+    if (rc != FS_OK) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return FS_OK;
+}
+
+fs_status fs_sim_destroy(fs_sim* sim) {
+    return fsb::guard([&] {
+        if (sim) {
+            cudaSetDevice(sim->impl.prm.device);
+            delete sim;
+        }
+    });
+}
+
+fs_status fs_sim_step(fs_sim* sim, int nsteps) {
+    return fsb::guard([&] {
+        if (!sim || nsteps < 0) fsb::fail(FS_ERR_ARG, "bad argument");
+        auto& S = sim->impl;
+        FS_CUDA(cudaSetDevice(S.prm.device));
+        S.step_ms.clear();
+        for (int k = 0; k < nsteps; ++k) {
+            FS_CUDA(cudaEventRecord(S.ev0, S.st));
+            S.step();
+            FS_CUDA(cudaEventRecord(S.ev1, S.st));
+            S.check_status();
+            float ms = 0.f;
+            FS_CUDA(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+            S.step_ms.push_back(ms);
+        }
+    });
+}
+
+fs_status fs_sim_remesh(fs_sim* sim) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
+        FS_CUDA(cudaSetDevice(sim->impl.prm.device));
+        sim->impl.remesh();
+        sim->impl.check_status();
+    });
+}
+
+fs_status fs_sim_num_points(const fs_sim* sim, int species, int* n) {
+    return fsb::guard([&] {
+        if (!sim || !n) fsb::fail(FS_ERR_ARG, "null argument");
+        if (species < 0) *n = sim->impl.N;
+        else if (species < (int)sim->impl.sp.size()) *n = sim->impl.sp[species]->n;
+        else fsb::fail(FS_ERR_ARG, "species out of range");
+    });
+}
+
+fs_status fs_sim_export(fs_sim* sim, double* xs, double* ps, double* fs, double* q_ws, double* es) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
+        auto& S = sim->impl;
+        FS_CUDA(cudaSetDevice(S.prm.device));
+        FS_CUDA(cudaStreamSynchronize(S.st));
+        const size_t b = sizeof(double) * S.N;
+        if (xs) FS_CUDA(cudaMemcpy(xs, S.x.p, b, cudaMemcpyDeviceToHost));
+        if (ps) FS_CUDA(cudaMemcpy(ps, S.p.p, b, cudaMemcpyDeviceToHost));
+        if (fs) FS_CUDA(cudaMemcpy(fs, S.f.p, b, cudaMemcpyDeviceToHost));
+        if (q_ws) FS_CUDA(cudaMemcpy(q_ws, S.qw.p, b, cudaMemcpyDeviceToHost));
+        if (es) FS_CUDA(cudaMemcpy(es, S.e.p, b, cudaMemcpyDeviceToHost));
+    });
+}
+
+fs_status fs_sim_import_xp(fs_sim* sim, const double* xs, const double* ps, const double* es) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
+        auto& S = sim->impl;
+        FS_CUDA(cudaSetDevice(S.prm.device));
+        FS_CUDA(cudaStreamSynchronize(S.st));
+        const size_t b = sizeof(double) * S.N;
+        if (xs) FS_CUDA(cudaMemcpy(S.x.p, xs, b, cudaMemcpyHostToDevice));
+        if (ps) FS_CUDA(cudaMemcpy(S.p.p, ps, b, cudaMemcpyHostToDevice));
+        if (es) FS_CUDA(cudaMemcpy(S.e.p, es, b, cudaMemcpyHostToDevice));
+    });
+}
+
+fs_status fs_sim_iter(const fs_sim* sim, int* iter, double* t) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
+        if (iter) *iter = sim->impl.iter;
+        if (t) *t = sim->impl.t;
+    });
+}
+
+fs_status fs_sim_step_times(const fs_sim* sim, double* ms, int cap, int* n) {
+    return fsb::guard([&] {
+        if (!sim || !n) fsb::fail(FS_ERR_ARG, "null argument");
+        const auto& v = sim->impl.step_ms;
+        const int k = std::min<int>((int)v.size(), std::max(cap, 0));
+        for (int i = 0; i < k && ms; ++i) ms[i] = v[i];
+        *n = k;
+    });
+}
+
+fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs) {
+    return fsb::guard([&] {
+        if (!sim || !pairs) fsb::fail(FS_ERR_ARG, "null argument");
+        *pairs = sim->impl.pairs;
+    });
+}
+
+}  // extern "C"

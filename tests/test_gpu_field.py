@@ -1,0 +1,102 @@
+"""GPU field kernels vs the reference (through the C ABI)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import multi_species_b200 as M
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL32 = 1e-6  # relative L2 bound on E for the FP32-compensated kernel
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "field_direct_*.npz"))))
+def test_direct64_bit_identical_to_reference_golden(path):
+    g = np.load(path)
+    f = M.E_MQ_DirectSum_B200(float(g["L"]), float(g["eps"]), "fp64")
+    e = f.evaluate(g["targets"], g["sources"], g["q"])
+    assert np.array_equal(e, g["es"])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "field_direct_*.npz"))))
+def test_direct32c_reference_golden(path):
+    g = np.load(path)
+    f = M.E_MQ_DirectSum_B200(float(g["L"]), float(g["eps"]), "fp32c")
+    e = f.evaluate(g["targets"], g["sources"], g["q"])
+    assert rel_l2(e, g["es"]) < TOL32
+
+
+def test_drop_in_call_signature_fills_es():
+    rng = np.random.default_rng(3)
+    L = 4 * np.pi
+    x = rng.uniform(0, L, 333)
+    q = rng.normal(size=333)
+    es = np.full(333, np.nan)
+    f = M.E_MQ_DirectSum_B200(L, 0.05)
+    f(es, x.copy(), 333, x.copy(), q, 333)
+    assert np.array_equal(es, O.direct_sum(L, 0.05, x, x, q))
+
+
+@pytest.mark.parametrize("n", [1, 2, 31, 513, 16770])
+def test_direct64_sizes_vs_oracle(n):
+    rng = np.random.default_rng(n)
+    L = 4 * np.pi
+    x = rng.uniform(-L, 2 * L, n)
+    q = rng.normal(size=n) * 1e-3
+    e = M.E_MQ_DirectSum_B200(L, 0.05, "fp64").evaluate(x, x, q)
+    assert np.array_equal(e, O.direct_sum(L, 0.05, x, x, q))
+
+
+@pytest.mark.parametrize("n,spread", [(1000, 1.0), (20000, 1.0), (20000, 3.0), (70000, 0.05)])
+def test_direct32c_vs_direct64(n, spread):
+    rng = np.random.default_rng(n + int(spread * 10))
+    L = 10 * np.pi
+    x = rng.uniform(-spread * L, spread * L, n) + L / 3
+    q = -np.abs(rng.normal(size=n)) * (L / n)
+    e64 = M.E_MQ_DirectSum_B200(L, 0.02, "fp64").evaluate(x, x, q)
+    e32 = M.E_MQ_DirectSum_B200(L, 0.02, "fp32c").evaluate(x, x, q)
+    assert rel_l2(e32, e64) < TOL32
+
+
+def test_direct32c_lattice_two_stream_scale():
+    """Full two-stream lattice (525,825 points), the precision form's workload:
+    FP32c vs the bit-exact FP64 GPU path."""
+    from multi_species_b200 import decks
+    d = decks.two_stream()
+    m = M.mesh(8, 1, 0.0, d["xmax"], -8.0, 8.0, q=-1.0, quadrature=0)
+    k = 2 * np.pi / d["xmax"]
+    f0 = (1 + 0.005 * np.cos(k * m["xs"])) * m["ps"] ** 2 * np.exp(-m["ps"] ** 2 / 2) / np.sqrt(2 * np.pi)
+    q = m["base_weights"] * f0
+    x = m["xs"] + 0.2 * m["ps"]  # one step of streaming
+    e64 = M.E_MQ_DirectSum_B200(d["xmax"], 0.02, "fp64").evaluate(x, x, q)
+    e32 = M.E_MQ_DirectSum_B200(d["xmax"], 0.02, "fp32c").evaluate(x, x, q)
+    assert rel_l2(e32, e64) < TOL32
+
+
+def test_empty_and_disjoint_sets():
+    L = 2.0
+    f32 = M.E_MQ_DirectSum_B200(L, 0.1, "fp32c")
+    f64 = M.E_MQ_DirectSum_B200(L, 0.1, "fp64")
+    t = np.linspace(0, 2, 7)
+    assert np.array_equal(f64.evaluate(t, np.zeros(0), np.zeros(0)), np.zeros(7))
+    assert np.array_equal(f32.evaluate(t, np.zeros(0), np.zeros(0)), np.zeros(7))
+    assert f32.evaluate(np.zeros(0), t, np.ones(7)).shape == (0,)
+    s = np.array([0.1, 0.5, 1.7])
+    qs = np.array([1.0, -2.0, 0.5])
+    assert rel_l2(f32.evaluate(t, s, qs), O.direct_sum(L, 0.1, t, s, qs)) < TOL32
+
+
+def test_uniform_lattice_field_vanishes():
+    """A uniform charge lattice has E = 0 at its points by symmetry."""
+    L = 2 * np.pi
+    x = np.arange(4096) * (L / 4096)
+    q = np.full(4096, 1.0 / 4096)
+    e = M.E_MQ_DirectSum_B200(L, 0.05, "fp32c").evaluate(x, x, q)
+    assert np.max(np.abs(e)) < 1e-9

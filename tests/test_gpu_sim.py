@@ -1,0 +1,97 @@
+"""Device-resident simulation vs the oracle restatement (through the C ABI)."""
+import numpy as np
+import pytest
+
+import oracle as O
+import multi_species_b200 as M
+from multi_species_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_initial_state_bit_identical():
+    d = decks.landau_two_species(h=4, ph=1)
+    g, o = M.Simulation(d), O.Sim(d)
+    a, b = g.state(), o.state()
+    for k in ("xs", "ps", "fs", "q_ws", "es"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_rk4_steps_bit_identical_before_remesh():
+    d = decks.landau_two_species(h=4, ph=1)
+    g, o = M.Simulation(d), O.Sim(d)
+    for _ in range(4):
+        g.step()
+        o.step()
+        a, b = g.state(), o.state()
+        for k in ("xs", "ps", "q_ws", "es"):
+            assert np.array_equal(a[k], b[k]), k
+
+
+def test_remesh_step_matches_oracle():
+    d = decks.landau_two_species(h=4, ph=1)
+    g, o = M.Simulation(d), O.Sim(d)
+    g.step(5)
+    o.step(5)
+    a, b = g.state(), o.state()
+    assert np.array_equal(a["xs"], b["xs"]) and np.array_equal(a["ps"], b["ps"])
+    assert rel(a["fs"], b["fs"]) < 1e-12
+    assert rel(a["q_ws"], b["q_ws"]) < 1e-12
+    assert rel(a["es"], b["es"]) < 1e-11
+
+
+def test_remesh_only_matches_oracle_interpolation():
+    """Remesh of a streamed two-stream state, species by species."""
+    d = decks.two_stream(h=5, ph=1, remesh_period=1000)
+    g, o = M.Simulation(d), O.Sim(d)
+    g.step(3)
+    o.step(3)
+    st = o.state()
+    m = O.Mesh(5, 1, d["xmin"], d["xmax"], -8.0, 8.0)
+    fmin = float(np.min(O.Sim(d).state()["fs"]))
+    nf, leaf, _ = m.remesh(st["xs"], st["ps"], st["fs"], fmin)
+    g.remesh()
+    a = g.state()
+    assert rel(a["fs"], nf) < 1e-12
+    assert np.array_equal(a["xs"], m.xs)
+
+
+def test_fp32c_session_field_error():
+    d = decks.two_stream(h=6, ph=1, remesh_period=5)
+    g64, g32 = M.Simulation(d, "direct64"), M.Simulation(d, "direct32c")
+    e0 = g64.state()["es"]
+    assert rel(g32.state()["es"], e0) < 1e-6
+    g64.step(2)
+    g32.step(2)
+    assert rel(g32.state()["es"], g64.state()["es"]) < 1e-6
+
+
+def test_field_energy_drift_fp32c_vs_fp64():
+    """Two-stream at reduced size (65 x 129 points), 100 steps with remesh every 5:
+    FP32c field energy within 1e-5 of the FP64 path over the whole run."""
+    d = decks.two_stream(h=5, ph=1, steps=100, remesh_period=5)
+    a, b = M.Simulation(d, "direct64"), M.Simulation(d, "direct32c")
+    L = d["xmax"]
+    wa, wb = [], []
+    for _ in range(100):
+        a.step()
+        b.step()
+        sa, sb = a.state(), b.state()
+        wa.append(O.field_energy(sa["xs"], sa["es"], L))
+        wb.append(O.field_energy(sb["xs"], sb["es"], L))
+    wa, wb = np.array(wa), np.array(wb)
+    assert np.max(np.abs(wb - wa)) / np.max(wa) < 1e-5
+
+
+def test_pair_count_and_launches():
+    d = decks.landau_two_species(h=3, ph=1)
+    n0 = M.kernel_launches()
+    g = M.Simulation(d)
+    g.step(1)
+    assert M.kernel_launches() > n0
+    n = g.n
+    assert g.pair_count() > 4 * n * n

@@ -1,0 +1,58 @@
+"""Host-side product code and the C ABI boundary (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+import multi_species_b200 as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "fs_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:fs_status|const char\*|int|long long)\s+(fs_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(M.LIB_PATH)
+    syms = header_symbols()
+    assert syms and sorted(M.EXPORTS) == syms
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+@pytest.mark.parametrize("h,ph,pmin,pmax", [(1, 0, -1.0, 1.0), (2, 1, -6.0, 6.0), (3, 2, -8.0, 8.0),
+                                            (5, 1, -6.0, 6.0), (6, 2, -10.0, 10.0)])
+@pytest.mark.parametrize("quad", [0, 1])
+def test_host_mesh_bit_identical_to_oracle(h, ph, pmin, pmax, quad):
+    L = 10 * np.pi
+    a = O.Mesh(h, ph, 0.0, L, pmin, pmax)
+    b = M.mesh(h, ph, 0.0, L, pmin, pmax, q=-0.9, quadrature=quad)
+    assert np.array_equal(a.xs, b["xs"]) and np.array_equal(a.ps, b["ps"])
+    assert np.array_equal(a.panels, b["panels"])
+    assert np.array_equal(a.leaves, b["leaves"])
+    assert np.array_equal(a.base_weights(-0.9, quad), b["base_weights"])
+
+
+def test_argument_errors_are_reported():
+    with pytest.raises(M.FsError) as ei:
+        M.mesh(0, 0, 0.0, 1.0, 0.0, 1.0)
+    assert ei.value.code == 1
+    with pytest.raises(M.FsError) as ei:
+        M.E_MQ_DirectSum_B200(-1.0, 0.1)
+    assert ei.value.code == 1
+    with pytest.raises(M.FsError) as ei:
+        M.sim_params(dict(bcs=1, species_list=[{}]))
+    assert ei.value.code == 8
+
+
+def test_no_cpu_fallback_without_library(tmp_path, monkeypatch):
+    monkeypatch.setattr(M, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(M, "_lib", None)
+    with pytest.raises(ImportError):
+        M.E_MQ_DirectSum_B200(1.0, 0.1)

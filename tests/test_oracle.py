@@ -1,0 +1,69 @@
+"""The oracle pinned against the reference: its own field solvers compiled from
+the reference sources (oracle/_ref) and the golden fixtures they produced."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from multi_species_b200 import decks
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "field_direct_*.npz"))))
+def test_direct_sum_matches_reference_golden_bitwise(path):
+    g = np.load(path)
+    e = O.direct_sum(float(g["L"]), float(g["eps"]), g["targets"], g["sources"], g["q"])
+    assert np.array_equal(e, g["es"])
+
+
+def test_treecode_matches_reference_golden_bitwise():
+    g = np.load(os.path.join(GOLD, "field_treecode.npz"))
+    e = O.treecode(float(g["L"]), float(g["eps"]), float(g["mac"]), int(g["degree"]), int(g["max_source"]),
+                   g["sources"], g["q"])
+    assert np.array_equal(e, g["es"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("n,spread,seed", [(1, 1.0, 0), (2, 1.0, 1), (257, 3.0, 2), (1500, 0.01, 3)])
+def test_direct_sum_live_reference(n, spread, seed):
+    rng = np.random.default_rng(seed)
+    L = 10 * np.pi
+    x = rng.uniform(-spread * L, spread * L, n)
+    x[: n // 3] = x[0]  # coincident points (z == 0 skipped)
+    q = rng.normal(size=n)
+    assert np.array_equal(O.direct_sum(L, 0.02, x, x, q), O.ref_direct_sum(L, 0.02, x, x, q))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("n,leaf,mac,deg", [(50, 2000, 0.7, 8), (3000, 200, 0.7, 8), (4000, 100, 0.5, 4)])
+def test_treecode_live_reference(n, leaf, mac, deg):
+    rng = np.random.default_rng(n)
+    L = 4 * np.pi
+    x = rng.uniform(-L, 2 * L, n)
+    q = rng.normal(size=n) * 1e-3
+    assert np.array_equal(O.treecode(L, 0.05, mac, deg, leaf, x, q), O.ref_treecode(L, 0.05, mac, deg, leaf, x, q))
+
+
+def test_treecode_normalisation_vs_direct():
+    """The reference treecode's kernel is the direct kernel times sqrt(L^2+4eps^2)/L."""
+    rng = np.random.default_rng(5)
+    L, eps = 4 * np.pi, 0.05
+    x = rng.uniform(0, L, 6000)
+    q = rng.normal(size=6000) * 1e-3
+    d = O.direct_sum(L, eps, x, x, q) * np.sqrt(L * L + 4 * eps * eps) / L
+    t = O.treecode(L, eps, 0.7, 8, 400, x, q)
+    assert np.linalg.norm(t - d) / np.linalg.norm(d) < 1e-5
+
+
+def test_sim_trajectory_golden():
+    g = np.load(os.path.join(GOLD, "sim_landau_h3.npz"))
+    s = O.Sim(decks.landau_two_species(h=3, ph=1, steps=6))
+    for k in range(7):
+        st = s.state()
+        for key in ("xs", "ps", "fs", "q_ws", "es"):
+            assert np.array_equal(st[key], g[f"{key}_{k}"]), (k, key)
+        if k < 6:
+            s.step()
