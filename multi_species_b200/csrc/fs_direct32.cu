@@ -16,16 +16,22 @@
 //    (sources before / after J_i take one of two images); the FP64 background
 //    term uses the same split, so both halves of the kernel agree exactly on
 //    which image a pair uses.
-//  * For a tile lying wholly on one side of the target (sigma = +-1) the pair
-//    kernel accumulates q/2 * (d*y - sigma) and adds sigma * sum(q/2) in FP64
-//    afterwards; the accumulated terms are then O(eps^2/d^2) instead of O(1),
-//    so FP32 accumulation error becomes negligible for far tiles.  Tiles near
-//    the target (sigma = 0) or straddling the image split use Kahan-compensated
-//    FP32 accumulation.  Every tile's partial sum is added into an FP64
-//    accumulator.
-//  * Per pair: FSUB, FFMA, MUFU.RSQ, FFMA, FFMA -- bound by the MUFU pipe
-//    (16 rsqrt/clk/SM), with source tiles moved global->shared by TMA bulk
-//    copies (cp.async.bulk, no multicast) double-buffered on mbarriers.
+//  * Per target the sources split into a far band (|d| > 12 eps) and a near
+//    band, by index (binary searches in FP64).  A far pair contributes
+//    sign(d) q/2 (1 - c(v)) with v = eps^2/(d^2+eps^2) <= 1/145: the sign(d) q/2
+//    part is summed exactly in FP64 from prefix sums of the FP64 charges; the
+//    pair kernel only
+//    accumulates q/2 * c(v), c = v/2 + v^2/8 + v^3/16 (series of 1-sqrt(1-v)),
+//    which is O(eps^2/d^2) and carries FP32's relative error on a small
+//    quantity.  Near-band pairs (|d| <= 12 eps, a few percent) use the full
+//    q/2 d*y with Kahan-compensated FP32 accumulation.  Every tile's partial
+//    sum is added into an FP64 accumulator.
+//  * Far pair: FSUB, FFMA, MUFU.RSQ, FMUL, FFMA, FFMA, FMUL, FFMA, the seven
+//    FP32 operations issued as packed FP32x2 instructions over two targets
+//    (Blackwell FADD2/FFMA2/FMUL2), so the MUFU pipe (16 rsqrt/clk/SM) and not
+//    the issue rate bounds the kernel, with source tiles
+//    moved global->shared by TMA bulk copies (cp.async.bulk, no multicast)
+//    double-buffered on mbarriers.
 //
 // Work is split over (target block, source chunk) CTAs; chunk partials are
 // summed in a fixed order by the finalize kernel, which also applies the fused
@@ -107,11 +113,11 @@ __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint6
     idx[i] = i;
 }
 
-// Sorted sources -> tile-relative FP32 records {s, q/2}; pads get {0, 0}.
-// Also the FP64 sorted q and q*x for the background sums.
+// Sorted sources -> tile-relative FP32 records {s, q/2} (pads {0, 0}), the
+// FP64 tile bases, and the FP64 q and q*x the exact sums are formed from.
 __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
                                  const double* __restrict__ q, int ns, int ns_pad, float2* __restrict__ src2,
-                                 double* __restrict__ qs, double* __restrict__ qx) {
+                                 double* __restrict__ tbase, double* __restrict__ qs, double* __restrict__ qx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns_pad) return;
     if (j >= ns) {
@@ -120,54 +126,67 @@ __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* 
     }
     const double xj = key_to_x(skeys[j]);
     const double base = key_to_x(skeys[(j / kS) * kS]);
+    if (j % kS == 0) tbase[j / kS] = base;
     const double qj = q[sidx[j]];
     src2[j] = make_float2((float)(xj - base), (float)(0.5 * qj));
     qs[j] = qj;
     qx[j] = qj * xj;
 }
 
-// Per tile: FP64 base, largest FP32 offset, and the FP64 sum of the FP32 q/2
-// actually used by the pair kernel (one warp per tile, fixed reduction order).
-__global__ void k_tile_stats(const float2* __restrict__ src2, const uint64_t* __restrict__ skeys, int ns,
-                             int ntiles, double* __restrict__ tbase, float* __restrict__ tsmax,
-                             double* __restrict__ tqh) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= ntiles) return;
-    const int j0 = warp * kS;
-    double s = 0.0;
-    for (int k = lane; k < kS; k += 32) s += (double)src2[j0 + k].y;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-        const int jl = min(ns - 1, j0 + kS - 1);
-        tbase[warp] = key_to_x(skeys[j0]);
-        tsmax[warp] = src2[jl].x;
-        tqh[warp] = s;
+// Position along the target's periodic window.  Sources are visited in the
+// cyclic order J, J+1, ..., n-1, 0, ..., J-1 ("unrolled" index u in [J, J+n));
+// X(u) = x_(u mod n) + L*(u >= n) increases with u and d(u) = tlo + L - X(u).
+__device__ __forceinline__ double unrolled_x(const uint64_t* __restrict__ skeys, int n, double L, int u) {
+    return (u >= n) ? key_to_x(skeys[u - n]) + L : key_to_x(skeys[u]);
+}
+__device__ __forceinline__ int unrolled_lower_bound(const uint64_t* __restrict__ skeys, int n, double L, int lo,
+                                                    int hi, double v, bool strict) {
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        const double xm = unrolled_x(skeys, n, L, mid);
+        if (strict ? (xm <= v) : (xm < v)) lo = mid + 1;
+        else hi = mid;
     }
+    return lo;
+}
+// exclusive prefix of the periodic extension: sum of w over unrolled [0, u)
+__device__ __forceinline__ double unrolled_prefix(const double* __restrict__ incl, int n, int u) {
+    const int k = u / n, r = u - k * n;
+    return k * incl[n - 1] + (r ? incl[r - 1] : 0.0);
 }
 
-// Per sorted target: its image split J (first source index whose periodic
-// image differs) and the target coordinate used for sources before J.
+struct TargetInfo {
+    double tlo;   // target coordinate for sources before J (after J: tlo + L)
+    double ffar;  // exact FP64 sum of sign(d) * q/2 over the far band (FP64 q)
+    int J, U1, U2;
+    int pad;
+};
+
+// Per sorted target: the image split J, the near band [U1, U2) in unrolled
+// index space (|d| <= band), and the far-band sign sum.
 __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt_pad,
-                              const uint64_t* __restrict__ skeys, int ns, double L, double* __restrict__ tlo,
-                              int* __restrict__ tJ) {
+                              const uint64_t* __restrict__ skeys, int ns, double L, double band,
+                              const double* __restrict__ pq, TargetInfo* __restrict__ info) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nt_pad) return;
+    TargetInfo T;
+    T.pad = 0;
     if (i >= nt) {
-        tlo[i] = 0.0;
-        tJ[i] = 0;
+        T.tlo = 0.0;
+        T.ffar = 0.0;
+        T.J = T.U1 = T.U2 = 0;
+        info[i] = T;
         return;
     }
     const double xw = key_to_x(tkeys[i]);
     const double half = 0.5 * L;
-    double th, shift;
+    double th;
     if (xw < half) {
         th = xw + half;   // sources at or beyond x_i + L/2 use the image +L
-        shift = 0.0;
+        T.tlo = xw;
     } else {
         th = xw - half;   // sources below x_i - L/2 use the image -L
-        shift = -L;
+        T.tlo = xw - L;
     }
     int lo = 0, hi = ns;
     while (lo < hi) {
@@ -175,20 +194,27 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
         if (key_to_x(skeys[mid]) < th) lo = mid + 1;
         else hi = mid;
     }
-    tJ[i] = lo;
-    tlo[i] = xw + shift;
+    T.J = lo;
+    const double c = T.tlo + L;  // d(u) = c - X(u)
+    T.U1 = unrolled_lower_bound(skeys, ns, L, T.J, T.J + ns, c - band, false);  // first d <= band
+    T.U2 = unrolled_lower_bound(skeys, ns, L, T.U1, T.J + ns, c + band, true);  // first d < -band
+    const double p_J = unrolled_prefix(pq, ns, T.J), p_1 = unrolled_prefix(pq, ns, T.U1);
+    const double p_2 = unrolled_prefix(pq, ns, T.U2), p_e = unrolled_prefix(pq, ns, T.J + ns);
+    T.ffar = 0.5 * ((p_1 - p_J) - (p_e - p_2));
+    info[i] = T;
 }
 
-template <int R>
-struct TileSetup {
-    float tau[R], tauh[R], nsg[R], sg[R];
-};
+// Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
+// v = eps^2 y^2 <= 1/(1 + kBand^2).  The sign part is summed in FP64 (ffar);
+// the pair kernel accumulates q/2 * c with c = z (a1 + z (a2 + z a3)),
+// z = y^2, a_k the series coefficients of 1 - sqrt(1 - v) times eps^(2k):
+// truncation error 5 v^3 / 64 relative, below FP32 rounding for kBand = 12.
+constexpr double kBand = 12.0;
 
 __global__ void __launch_bounds__(kNT)
-k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, const float* __restrict__ tsmax,
-          const double* __restrict__ tqh, int ntiles, int tiles_per_chunk, const double* __restrict__ tlo,
-          const int* __restrict__ tJ, int nt_pad, double L, float eps2, double* __restrict__ partial,
-          int* __restrict__ err) {
+k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int ns, int ntiles,
+          int tiles_per_chunk, const TargetInfo* __restrict__ info, int nt_pad, double L, float eps2, float a1,
+          float a2, float a3, double* __restrict__ partial, int* __restrict__ err) {
     __shared__ __align__(128) float2 buf[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
     const int tid = threadIdx.x;
@@ -197,12 +223,14 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, con
     if (t0 >= t1) return;
     const int ibase = blockIdx.x * kTB + tid;
     double tl[kR], acc64[kR];
-    int J[kR];
+    int J[kR], U1[kR], U2[kR];
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-        const int i = ibase + r * kNT;  // nt_pad is a multiple of kTB: always in range
-        tl[r] = tlo[i];
-        J[r] = tJ[i];
+        const TargetInfo T = info[ibase + r * kNT];  // nt_pad is a multiple of kTB
+        tl[r] = T.tlo;
+        J[r] = T.J;
+        U1[r] = T.U1;
+        U2[r] = T.U2;
         acc64[r] = 0.0;
     }
     if (tid == 0) {
@@ -234,43 +262,61 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, con
             return;
         }
         const double base = tbase[t];
-        const float smax = tsmax[t];
         const int jlo = t * kS;
-        float tau[kR], tauh[kR], nsg[kR], sg[kR], acc[kR];
+        const int jend = min(jlo + kS, ns);  // real sources in this tile
+        float tau[kR], tauh[kR], sg[kR], acc[kR];
         bool careful = false;
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
             const double lo = tl[r] - base;
-            const bool all_lo = (jlo + kS <= J[r]);
-            const bool all_hi = (jlo >= J[r]);
-            const float a = (float)(all_hi ? lo + L : lo);
-            tau[r] = a;
-            tauh[r] = (all_lo || all_hi) ? a : (float)(lo + L);
+            tau[r] = (float)lo;
+            tauh[r] = (float)(lo + L);
             float s = 0.f;
-            if (all_lo || all_hi) s = (a > smax) ? 1.f : ((a < 0.f) ? -1.f : 0.f);
+            if (jend <= J[r]) {          // whole tile on the lo image: u = j + n
+                if (jend + ns <= U1[r]) s = 1.f;
+                else if (jlo + ns >= U2[r]) s = -1.f;
+            } else if (jlo >= J[r]) {    // whole tile on the hi image: u = j
+                tau[r] = tauh[r];
+                if (jend <= U1[r]) s = 1.f;
+                else if (jlo >= U2[r]) s = -1.f;
+            }
             sg[r] = s;
-            nsg[r] = -s;
             acc[r] = 0.f;
             careful |= (s == 0.f);
         }
         const float2* tile = buf[b];
         if (!__any_sync(0xffffffffu, careful)) {
-            // far tiles: every lane's tile lies on one side of its targets
+            // far tiles: accumulate q/2 * c(v), two targets per packed FP32x2 op
+            const float2 e2v = make_float2(eps2, eps2), a1v = make_float2(a1, a1);
+            const float2 a2v = make_float2(a2, a2), a3v = make_float2(a3, a3);
+            float2 tau2[kR / 2], acc2[kR / 2];
+#pragma unroll
+            for (int h = 0; h < kR / 2; ++h) {
+                tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
+                acc2[h] = make_float2(0.f, 0.f);
+            }
 #pragma unroll 4
             for (int j = 0; j < kS; ++j) {
                 const float2 e = tile[j];
+                const float2 ns = make_float2(-e.x, -e.x), qh = make_float2(e.y, e.y);
 #pragma unroll
-                for (int r = 0; r < kR; ++r) {
-                    const float d = tau[r] - e.x;
-                    const float y = rsqrt_approx(fmaf(d, d, eps2));
-                    const float u = fmaf(d, y, nsg[r]);
-                    acc[r] = fmaf(e.y, u, acc[r]);
+                for (int h = 0; h < kR / 2; ++h) {
+                    const float2 d = __fadd2_rn(tau2[h], ns);
+                    const float2 r2 = __ffma2_rn(d, d, e2v);
+                    const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    const float2 z = __fmul2_rn(y, y);
+                    const float2 p = __ffma2_rn(z, __ffma2_rn(z, a3v, a2v), a1v);
+                    acc2[h] = __ffma2_rn(qh, __fmul2_rn(z, p), acc2[h]);
                 }
             }
 #pragma unroll
-            for (int r = 0; r < kR; ++r) acc64[r] += (double)acc[r] + (double)sg[r] * tqh[t];
+            for (int h = 0; h < kR / 2; ++h) {
+                acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].x;
+                acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].y;
+            }
         } else {
-            // near / image-split tiles: per-pair image, Kahan-compensated sum
+            // near band / image split: per-pair image and band, Kahan sum of
+            // q/2 * d*y (near) or -+ q/2 * c (far)
             float cmp[kR];
 #pragma unroll
             for (int r = 0; r < kR; ++r) cmp[r] = 0.f;
@@ -279,19 +325,21 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, con
                 const int idx = jlo + j;
 #pragma unroll
                 for (int r = 0; r < kR; ++r) {
-                    const float tr = (idx < J[r]) ? tau[r] : tauh[r];
-                    const float d = tr - e.x;
+                    const bool lo_img = idx < J[r];
+                    const int u = lo_img ? idx + ns : idx;
+                    const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
                     const float y = rsqrt_approx(fmaf(d, d, eps2));
-                    const float u = fmaf(d, y, nsg[r]);
-                    const float v = fmaf(e.y, u, -cmp[r]);
-                    const float s = acc[r] + v;
-                    cmp[r] = (s - acc[r]) - v;
-                    acc[r] = s;
+                    const float z = y * y;
+                    const float c = z * fmaf(z, fmaf(z, a3, a2), a1);
+                    const float val = (u < U1[r]) ? -c : ((u >= U2[r]) ? c : d * y);
+                    const float v = fmaf(e.y, val, -cmp[r]);
+                    const float sum = acc[r] + v;
+                    cmp[r] = (sum - acc[r]) - v;
+                    acc[r] = sum;
                 }
             }
 #pragma unroll
-            for (int r = 0; r < kR; ++r)
-                acc64[r] += ((double)acc[r] - (double)cmp[r]) + (double)sg[r] * tqh[t];
+            for (int r = 0; r < kR; ++r) acc64[r] += (double)acc[r] - (double)cmp[r];
         }
         __syncthreads();
     }
@@ -300,21 +348,23 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, con
     for (int r = 0; r < kR; ++r) out[ibase + r * kNT] = acc64[r];
 }
 
-// Sum the chunk partials in a fixed order, subtract the FP64 background and
-// apply the stage epilogue at the target's original index.
+// Sum the chunk partials in a fixed order, add the exact far-band sign sum,
+// subtract the FP64 background and apply the stage epilogue at the target's
+// original index.
 __global__ void k_finalize32(const double* __restrict__ partial, int nchunks, int nt_pad, int nt,
-                             const double* __restrict__ tlo, const int* __restrict__ tJ,
-                             const double* __restrict__ pq, const double* __restrict__ qxsum, int ns, double L,
-                             double cbg, const int* __restrict__ tperm, Stage S) {
+                             const TargetInfo* __restrict__ info, const double* __restrict__ pq,
+                             const double* __restrict__ qxsum, int ns, double L, double cbg,
+                             const int* __restrict__ tperm, Stage S) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nt) return;
     double E = 0.0;
     for (int c = 0; c < nchunks; ++c) E += partial[(size_t)c * nt_pad + i];
     if (ns > 0) {
+        const TargetInfo T = info[i];
         const double Q = pq[ns - 1];
-        const int J = tJ[i];
-        const double PJ = (J > 0) ? pq[J - 1] : 0.0;
-        const double B = tlo[i] * Q - qxsum[0] + L * (Q - PJ);
+        const double PJ = (T.J > 0) ? pq[T.J - 1] : 0.0;
+        const double B = T.tlo * Q - qxsum[0] + L * (Q - PJ);
+        E += T.ffar;
         E -= cbg * B;
     }
     apply_stage(S, tperm[i], E);
@@ -347,15 +397,13 @@ class Direct32c final : public FieldEngine {
             k_wrap_keys<<<(ns + T - 1) / T, T, 0, st>>>(d_s, ns, L_, kin_.p, iin_.p);
             size_t tb = cub_.bytes();
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
-            k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, src2_.p, qs_.p,
-                                                                 qx_.p);
-            k_tile_stats<<<(ntiles * 32 + T - 1) / T, T, 0, st>>>(src2_.p, kout_.p, ns, ntiles, tbase_.p, tsmax_.p,
-                                                                  tqh_.p);
+            k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, src2_.p,
+                                                                 tbase_.p, qs_.p, qx_.p);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
-            FS_LAUNCHED(3);  // own kernels (the sort / scan / reduce kernels are CUB's)
+            FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
         }
         if (same) {
             tkeys = kout_.p;
@@ -369,18 +417,21 @@ class Direct32c final : public FieldEngine {
             FS_LAUNCHED(1);
         }
         if (ns > 0) {
-            k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, tlo_.p, tJ_.p);
+            k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_,
+                                                             pq_.p, info_.p);
             dim3 grid(tblocks, nchunks);
+            const double e2 = eps_ * eps_;
             ProfScope prof("k_pairs32", st, last_pairs);
-            k_pairs32<<<grid, kNT, 0, st>>>(src2_.p, tbase_.p, tsmax_.p, tqh_.p, ntiles, tpc, tlo_.p, tJ_.p, nt_pad,
-                                             L_, (float)(eps_ * eps_), partial_.p, err_.p);
+            k_pairs32<<<grid, kNT, 0, st>>>(src2_.p, tbase_.p, ns, ntiles, tpc, info_.p, nt_pad, L_, (float)e2,
+                                             (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(e2 * e2 * e2 / 16),
+                                             partial_.p, err_.p);
             FS_LAUNCHED(2);
         } else {
             FS_CUDA(cudaMemsetAsync(partial_.p, 0, sizeof(double) * nt_pad, st));
             nchunks = 1;
         }
-        k_finalize32<<<(nt + T - 1) / T, T, 0, st>>>(partial_.p, nchunks, nt_pad, nt, tlo_.p, tJ_.p, pq_.p,
-                                                      qxsum_.p, ns, L_, cbg_, tperm, stage);
+        k_finalize32<<<(nt + T - 1) / T, T, 0, st>>>(partial_.p, nchunks, nt_pad, nt, info_.p, pq_.p, qxsum_.p, ns,
+                                                      L_, cbg_, tperm, stage);
         FS_LAUNCHED(1);
     }
 
@@ -398,10 +449,7 @@ class Direct32c final : public FieldEngine {
         pq_.ensure(ns);
         qxsum_.ensure(1);
         tbase_.ensure(std::max(ntiles, 1));
-        tsmax_.ensure(std::max(ntiles, 1));
-        tqh_.ensure(std::max(ntiles, 1));
-        tlo_.ensure(nt_pad);
-        tJ_.ensure(nt_pad);
+        info_.ensure(nt_pad);
         partial_.ensure(npartial);
         if (!err_.p) {
             err_.ensure(1);
@@ -429,9 +477,9 @@ class Direct32c final : public FieldEngine {
     DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float2> src2_;
-    DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, tqh_, tlo_, partial_;
-    DevBuf<float> tsmax_;
-    DevBuf<int> tJ_, err_;
+    DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
+    DevBuf<TargetInfo> info_;
+    DevBuf<int> err_;
     DevBuf<unsigned char> cub_;
 };
 

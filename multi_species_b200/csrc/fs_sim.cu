@@ -11,12 +11,17 @@
 // Remesh per species (AMRStructure::remesh, AMRStructure_amr.cpp:1156-1202):
 //   k_panel_fit    one thread per old leaf: 9x9 LU fit of f about point 4
 //                  (interpolate_from_panel_to_points, AMRStructure_interp.cpp:795-975)
-//   k_locate_eval  one thread per new lattice point: periodic shift into the
-//                  sheared root (shift_xs :429-491), start at the panel the
-//                  point's material came from, then the reference's neighbour
-//                  walk (find_leaf_containing_point_from_neighbor :12-230) with
-//                  its half-open edge tests, bounded; evaluate the fit or
-//                  f_beyond_boundary.
+//   k_shift        per point: periodic shift into the sheared root (shift_xs :429-491)
+//   k_row_sort     per lattice row (one CTA): sort by shifted x, the order the
+//                  reference's global sort gives (:525-558)
+//   k_walk_first_column / k_walk_rows
+//                  the reference's neighbour walk (find_leaf_containing_point_from_neighbor
+//                  :12-230) in the reference's order: first point from the root,
+//                  the first column sequentially, then one thread per row, each
+//                  walk starting at the previous point's leaf.  In a strongly
+//                  deformed (tangled) mesh a point can lie in more than one old
+//                  panel, and only this order reproduces the reference's choice.
+//   k_eval_points  per point: the located panel's fit or f_beyond_boundary
 //   k_reset_points x,p <- lattice, f <- new f, q_w <- w0 * f
 //                  (set_leaves_weights :1084-1151 with cached w0).
 // Reduced grid (evaluate_field_uniform_grid, AMRSimulation_field.cpp:5-162,
@@ -25,6 +30,7 @@
 // per-column charge sums (in the reference's summation order) are formed.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <memory>
 
@@ -132,14 +138,12 @@ __global__ void k_panel_fit(int nleaves, const int* __restrict__ leaves, const i
 struct MeshView {
     const int* rec;        // 18 ints per panel
     const int* leaf_slot;  // panel -> leaf slot (or -1)
-    const int* cell_leaf;  // (ix * npp + ip) -> leaf panel of the lattice cell
     const double* lat_x;
     const double* lat_p;
     const double* coef;
     int npx, npp, n;
     double xmin, pmin, Lx, dxp, dpp;
     double f_beyond;
-    double shear_t;        // time since the mesh was last reset (start guess)
 };
 
 __device__ __forceinline__ bool edge_right(double x_tr, double p_tr, double x_br, double p_br, double tx, double tp) {
@@ -155,50 +159,22 @@ __device__ __forceinline__ bool edge_bottom(double x_br, double p_br, double x_b
     return dmul(dsub(x_br, x_bl), dsub(tp, p_bl)) >= dmul(dsub(p_br, p_bl), dsub(tx, x_bl));
 }
 
-__global__ void k_locate_eval(MeshView M, const double* __restrict__ ox, const double* __restrict__ op,
-                              double* __restrict__ fnew, int* __restrict__ status) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= M.n) return;
-    const double tp = M.lat_p[k];
-    double tx = M.lat_x[k];
+// find_leaf_containing_point_from_neighbor (AMRStructure_interp.cpp:12-230):
+// starting at `leaf`, apply the half-open edge tests of the current panel and
+// step to the neighbour across the first failed edge (right, top, bottom, left
+// priority), shifting tx by Lx across the periodic seam; stop at the first
+// panel already visited.  beyond_boundary is or-ed over every visited panel.
+// Bounded: returns -1 when the walk exceeds kWalkLimit steps.
+__device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const double* __restrict__ op,
+                         double& tx, double tp, int leaf, bool& beyond) {
     const double Lx = M.Lx;
-    // shift_xs: into the sheared root panel (old points 0, 2, 6, 8)
-    {
-        const double x_bl = ox[0], p_bl = op[0], x_tl = ox[2], p_tl = op[2];
-        const double x_br = ox[6], p_br = op[6], x_tr = ox[8], p_tr = op[8];
-        int cnt = 0;
-        while (!edge_left(x_tl, p_tl, x_bl, p_bl, tx, tp)) {
-            tx = dadd(tx, Lx);
-            if (++cnt > 10) {
-                raise_status(status, FS_ERR_SHIFT);
-                return;
-            }
-        }
-        cnt = 0;
-        while (!edge_right(x_tr, p_tr, x_br, p_br, tx, tp)) {
-            tx = dsub(tx, Lx);
-            if (++cnt > 10) {
-                raise_status(status, FS_ERR_SHIFT);
-                return;
-            }
-        }
-    }
-    // start at the panel whose material streamed to this point
-    double xg = tx - tp * M.shear_t - M.xmin;
-    xg -= Lx * floor(xg / Lx);
-    int ix = (int)floor(xg / M.dxp);
-    ix = min(max(ix, 0), M.npx - 1);
-    int ip = (int)floor((tp - M.pmin) / M.dpp);
-    ip = min(max(ip, 0), M.npp - 1);
-    int leaf = M.cell_leaf[ix * M.npp + ip];
+    const int* R = M.rec;
     int hist[kHist];
     int nh = 0;
     hist[nh++] = leaf;
-    bool beyond = false;
-    int steps = 0;
-    const int* R = M.rec;
-    for (;;) {
-        if (leaf == 0) break;
+    for (int steps = 0;; ++steps) {
+        if (leaf == 0) return 0;
+        if (steps > kWalkLimit) return -1;
         const int* P = R + (size_t)leaf * 18;
         const double x_bl = ox[P[0]], p_bl = op[P[0]];
         const double x_tl = ox[P[2]], p_tl = op[P[2]];
@@ -232,28 +208,251 @@ __global__ void k_locate_eval(MeshView M, const double* __restrict__ ox, const d
             beyond = true;
         bool seen = false;
         for (int h = 0; h < min(nh, kHist); ++h) seen |= (hist[h] == nl);
-        leaf = nl;
-        if (seen) break;
+        if (seen) return nl;
         hist[nh % kHist] = nl;
         ++nh;
-        if (++steps > kWalkLimit) {
+        leaf = nl;
+    }
+}
+
+// find_leaf_containing_xp_recursively (AMRStructure_interp.cpp:232-426), used
+// for the first point only; x is updated in place as in the reference.
+__device__ int find_from_root(const MeshView& M, const double* __restrict__ ox, const double* __restrict__ op,
+                              double& x, double p, bool& beyond) {
+    const int* R = M.rec;
+    const double Lx = M.Lx;
+    int pi = 0;
+    for (int depth = 0; depth < 64; ++depth) {
+        const int* P = R + (size_t)pi * 18;
+        const int flags = P[17], cs = P[12];
+        const bool xp = flags & 4, pr = flags & 8;
+        if (!(xp || pr)) {
+            const double x_bl = ox[P[0]], p_bl = op[P[0]], x_tl = ox[P[2]], p_tl = op[P[2]];
+            const double x_br = ox[P[6]], p_br = op[P[6]], x_tr = ox[P[8]], p_tr = op[P[8]];
+            const bool ir = edge_right(x_tr, p_tr, x_br, p_br, x, p);
+            const bool il = edge_left(x_tl, p_tl, x_bl, p_bl, x, p);
+            const bool it = edge_top(x_tr, p_tr, x_tl, p_tl, x, p);
+            const bool ib = edge_bottom(x_br, p_br, x_bl, p_bl, x, p);
+            if ((!il && P[13] == -2) || (!ir && P[15] == -2) || (!it && P[14] == -2) || (!ib && P[16] == -2))
+                beyond = true;
+            return pi;
+        }
+        double xc[9], pc[9];
+        for (int i = 0; i < 9; ++i) {
+            xc[i] = ox[P[i]];
+            pc[i] = op[P[i]];
+        }
+        // a >= b  <=>  (xa - xb)*(p - pb) >= (pa - pb)*(x - xb) style tests on the panel's mid lines
+        auto ge = [&](int a, int b) { return dmul(dsub(xc[a], xc[b]), dsub(p, pc[b])) >= dmul(dsub(pc[a], pc[b]), dsub(x, xc[b])); };
+        auto le = [&](int a, int b) { return dmul(dsub(xc[a], xc[b]), dsub(p, pc[b])) <= dmul(dsub(pc[a], pc[b]), dsub(x, xc[b])); };
+        const bool i1b = ge(4, 1), i1r = ge(5, 4), i3b = ge(7, 4);
+        const int* C = R;
+        int sub;
+        if (i1b && i1r) {
+            const int c1 = cs + 1;
+            const bool i1t = le(5, 2);
+            if (i1t || C[(size_t)c1 * 18 + 14] < 0) {
+                const bool i1l = le(2, 1);
+                if (i1l || C[(size_t)c1 * 18 + 13] < 0) sub = c1;
+                else {
+                    sub = C[(size_t)c1 * 18 + 13];
+                    if (flags & 1) x = dadd(x, Lx);
+                }
+            } else sub = C[(size_t)c1 * 18 + 14];
+        } else if (i3b && !i1r) {
+            const int c3 = pr ? cs + 1 : cs + 3;
+            const bool i3t = le(8, 5);
+            if (i3t || C[(size_t)c3 * 18 + 14] < 0) {
+                const bool i3r = le(8, 7);
+                if (!i3r || C[(size_t)c3 * 18 + 15] < 0) sub = c3;
+                else {
+                    sub = C[(size_t)c3 * 18 + 15];
+                    if (flags & 2) x = dsub(x, Lx);
+                }
+            } else sub = C[(size_t)c3 * 18 + 14];
+        } else {
+            const bool i0r = ge(4, 3);
+            if (i0r) {
+                const int c0 = cs;
+                const bool i0b = ge(3, 0);
+                if (i0b || C[(size_t)c0 * 18 + 16] < 0) {
+                    const bool i0l = le(1, 0);
+                    if (i0l || C[(size_t)c0 * 18 + 13] < 0) sub = c0;
+                    else {
+                        sub = C[(size_t)c0 * 18 + 13];
+                        if (flags & 1) x = dadd(x, Lx);
+                    }
+                } else sub = C[(size_t)c0 * 18 + 16];
+            } else {
+                const int c2 = pr ? cs : cs + 2;
+                const bool i2b = ge(6, 3);
+                if (i2b || C[(size_t)c2 * 18 + 16] < 0) {
+                    const bool i2r = le(7, 6);
+                    if (!i2r || C[(size_t)c2 * 18 + 15] < 0) sub = c2;
+                    else {
+                        sub = C[(size_t)c2 * 18 + 15];
+                        if (flags & 2) x = dsub(x, Lx);
+                    }
+                } else sub = C[(size_t)c2 * 18 + 16];
+            }
+        }
+        pi = sub;
+    }
+    return -1;
+}
+
+// shift_xs (AMRStructure_interp.cpp:429-491): lattice x -> the periodic image
+// inside the sheared root panel (old points 0, 2, 6, 8).
+__global__ void k_shift(int n, const double* __restrict__ lat_x, const double* __restrict__ lat_p, double Lx,
+                        const double* __restrict__ ox, const double* __restrict__ op, double* __restrict__ sx,
+                        int* __restrict__ status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double tp = lat_p[k];
+    double tx = lat_x[k];
+    const double x_bl = ox[0], p_bl = op[0], x_tl = ox[2], p_tl = op[2];
+    const double x_br = ox[6], p_br = op[6], x_tr = ox[8], p_tr = op[8];
+    int cnt = 0;
+    while (!edge_left(x_tl, p_tl, x_bl, p_bl, tx, tp)) {
+        tx = dadd(tx, Lx);
+        if (++cnt > 10) {
+            raise_status(status, FS_ERR_SHIFT);
+            break;
+        }
+    }
+    cnt = 0;
+    while (!edge_right(x_tr, p_tr, x_br, p_br, tx, tp)) {
+        tx = dsub(tx, Lx);
+        if (++cnt > 10) {
+            raise_status(status, FS_ERR_SHIFT);
+            break;
+        }
+    }
+    sx[k] = tx;
+}
+
+// The reference sorts all points by p row, then shifted x (AMRStructure_interp.cpp:525-558).
+// Lattice rows are separated by far more than the sort threshold, so this is a
+// per-row sort by (shifted x, point index): one CTA per row, bitonic sort in
+// shared memory.  Writes sorted x, p and the point index of each sorted slot.
+__global__ void k_row_sort(int nx, int pow2, const int* __restrict__ row_pts, const double* __restrict__ sx,
+                           const double* __restrict__ lat_p, double* __restrict__ sortx, double* __restrict__ sortp,
+                           int* __restrict__ order) {
+    extern __shared__ unsigned char smem_raw[];
+    double* kx = reinterpret_cast<double*>(smem_raw);
+    int* ki = reinterpret_cast<int*>(kx + pow2);
+    const int row = blockIdx.x;
+    for (int t = threadIdx.x; t < pow2; t += blockDim.x) {
+        if (t < nx) {
+            const int pt = row_pts[(size_t)row * nx + t];
+            kx[t] = sx[pt];
+            ki[t] = pt;
+        } else {
+            kx[t] = INFINITY;
+            ki[t] = INT_MAX;
+        }
+    }
+    __syncthreads();
+    for (int size = 2; size <= pow2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < pow2; t += blockDim.x) {
+                const int u = t ^ stride;
+                if (u > t) {
+                    const bool up = ((t & size) == 0);
+                    const bool gt = (kx[t] > kx[u]) || (kx[t] == kx[u] && ki[t] > ki[u]);
+                    if (gt == up) {
+                        const double a = kx[t];
+                        kx[t] = kx[u];
+                        kx[u] = a;
+                        const int b = ki[t];
+                        ki[t] = ki[u];
+                        ki[u] = b;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int t = threadIdx.x; t < nx; t += blockDim.x) {
+        const size_t o = (size_t)row * nx + t;
+        sortx[o] = kx[t];
+        sortp[o] = lat_p[ki[t]];
+        order[o] = ki[t];
+    }
+}
+
+// First point from the root, then the first column row by row, each walk
+// starting where the previous one ended (AMRStructure_interp.cpp:608-650).
+// One thread: the reference's dependency chain.
+__global__ void k_walk_first_column(MeshView M, int nx, int np, const double* __restrict__ ox,
+                                    const double* __restrict__ op, double* __restrict__ sortx,
+                                    const double* __restrict__ sortp, int* __restrict__ first_col,
+                                    int* __restrict__ leaf_of, int* __restrict__ status) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    bool beyond = false;
+    int leaf = find_from_root(M, ox, op, sortx[0], sortp[0], beyond);
+    if (leaf < 0) {
+        raise_status(status, FS_ERR_WALK);
+        return;
+    }
+    for (int ii = 0; ii < np; ++ii) {
+        const int pt = ii * nx;
+        beyond = false;
+        double tx = sortx[pt];
+        leaf = walk_from(M, ox, op, tx, sortp[pt], leaf, beyond);
+        if (leaf < 0) {
             raise_status(status, FS_ERR_WALK);
             return;
         }
+        sortx[pt] = tx;
+        first_col[ii] = leaf;
+        leaf_of[pt] = beyond ? 0 : leaf;
     }
-    double v;
+}
+
+// Every row: walk its sorted points left to right, each from the previous
+// point's leaf (AMRStructure_interp.cpp:689-722).  One thread per row.
+__global__ void k_walk_rows(MeshView M, int nx, int np, const double* __restrict__ ox, const double* __restrict__ op,
+                            double* __restrict__ sortx, const double* __restrict__ sortp,
+                            const int* __restrict__ first_col, int* __restrict__ leaf_of, int* __restrict__ status) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= np) return;
+    int lc = first_col[ii];
+    for (int jj = 1; jj < nx; ++jj) {
+        const int pt = ii * nx + jj;
+        bool beyond = false;
+        double tx = sortx[pt];
+        lc = walk_from(M, ox, op, tx, sortp[pt], lc, beyond);
+        if (lc < 0) {
+            raise_status(status, FS_ERR_WALK);
+            return;
+        }
+        sortx[pt] = tx;
+        leaf_of[pt] = beyond ? 0 : lc;
+    }
+}
+
+// Evaluate the located panel's fit (or f_beyond_boundary) at every sorted
+// slot and scatter back to point order.
+__global__ void k_eval_points(MeshView M, const double* __restrict__ sortx, const double* __restrict__ sortp,
+                              const int* __restrict__ order, const int* __restrict__ leaf_of,
+                              double* __restrict__ fnew) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= M.n) return;
+    const int leaf = leaf_of[k];
     const int slot = (leaf > 0) ? M.leaf_slot[leaf] : -1;
-    if (beyond || leaf == 0 || slot < 0) {
+    double v;
+    if (slot < 0) {
         v = M.f_beyond;
     } else {
         const double* c = M.coef + (size_t)slot * 11;
-        const double dx = dsub(tx, c[9]), dp = dsub(tp, c[10]);
+        const double dx = dsub(sortx[k], c[9]), dp = dsub(sortp[k], c[10]);
         const double dxsq = dmul(dx, dx), dpsq = dmul(dp, dp);
         const double D[9] = {1.0, dx, dmul(dx, dp), dp, dxsq, dmul(dxsq, dp), dmul(dxsq, dpsq), dmul(dx, dpsq), dpsq};
         v = 0.0;
         for (int j = 0; j < 9; ++j) v = dadd(v, dmul(D[j], c[j]));
     }
-    fnew[k] = v;
+    fnew[order[k]] = v;
 }
 
 __global__ void k_reset_points(int n, const double* __restrict__ lat_x, const double* __restrict__ lat_p,
@@ -290,7 +489,7 @@ void upload(DevBuf<T>& b, const std::vector<T>& h) {
     if (!h.empty()) FS_CUDA(cudaMemcpy(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
 }
 
-inline int blocks(int n) { return (n + kT - 1) / kT; }
+inline int blocks(int n, int per = kT) { return (n + per - 1) / per; }
 
 }  // namespace
 
@@ -300,7 +499,10 @@ struct SpeciesState {
     double q = 0, m = 0, qm = 0, f_beyond = 0;
     int nleaves = 0, npx = 0, npp = 0;
     DevBuf<double> lat_x, lat_p, w0, coef, fnew;
-    DevBuf<int> rec, leaf_slot, leaves, cell_leaf;
+    DevBuf<int> rec, leaf_slot, leaves, row_pts;
+    DevBuf<double> sx, sortx, sortp;
+    DevBuf<int> order, leaf_of, first_col;
+    int nxl = 0, npl = 0, pow2 = 1;
     // reduced grid
     int nu = 0, roff = 0;
     DevBuf<int> inv, col_off, col_idx;
@@ -309,7 +511,7 @@ struct SpeciesState {
 struct Sim {
     fs_sim_params prm{};
     int N = 0, U = 0, iter = 0;
-    double L = 0, t = 0, t_reset = 0, pairs = 0;
+    double L = 0, t = 0, pairs = 0;
     std::vector<std::unique_ptr<SpeciesState>> sp;
     DevBuf<double> x, p, f, qw, e, xkA, xkB, pst, accX, accP, rx, rw, re;
     DevBuf<int> status;
@@ -395,18 +597,30 @@ struct Sim {
             std::vector<int> slot(M.panels.size(), -1);
             for (size_t l = 0; l < M.leaves.size(); ++l) slot[M.leaves[l]] = (int)l;
             upload(ss->leaf_slot, slot);
-            // lattice cell -> leaf panel, from each leaf's lower-left corner
-            std::vector<int> cell((size_t)ss->npx * ss->npp, 0);
-            const double dxp = L / ss->npx, dpp = (S.pmax - S.pmin) / ss->npp;
-            for (int l : M.leaves) {
-                const int c0 = M.panels[l].pts[0];
-                int ix = (int)std::lround((M.xs[c0] - P.xmin) / dxp);
-                int ip = (int)std::lround((M.ps[c0] - S.pmin) / dpp);
-                ix = std::min(std::max(ix, 0), ss->npx - 1);
-                ip = std::min(std::max(ip, 0), ss->npp - 1);
-                cell[(size_t)ix * ss->npp + ip] = l;
+            // lattice rows (ascending p), each listing its points by column
+            ss->nxl = M.nx();
+            ss->npl = M.np();
+            {
+                const double hx = L / ss->npx / 2, hp = (S.pmax - S.pmin) / ss->npp / 2;
+                std::vector<int> rows((size_t)ss->nxl * ss->npl, -1);
+                for (int i = 0; i < ss->n; ++i) {
+                    const int c = (int)std::lround((M.xs[i] - P.xmin) / hx);
+                    const int r = (int)std::lround((M.ps[i] - S.pmin) / hp);
+                    if (c < 0 || c >= ss->nxl || r < 0 || r >= ss->npl || rows[(size_t)r * ss->nxl + c] != -1)
+                        fail(FS_ERR_STATE, "mesh points do not form the expected lattice");
+                    rows[(size_t)r * ss->nxl + c] = i;
+                }
+                upload(ss->row_pts, rows);
             }
-            upload(ss->cell_leaf, cell);
+            while (ss->pow2 < ss->nxl) ss->pow2 <<= 1;
+            if ((size_t)ss->pow2 * (sizeof(double) + sizeof(int)) > 200 * 1024)
+                fail(FS_ERR_UNSUPPORTED, "mesh rows longer than the row sort supports");
+            ss->sx.ensure(ss->n);
+            ss->sortx.ensure(ss->n);
+            ss->sortp.ensure(ss->n);
+            ss->order.ensure(ss->n);
+            ss->leaf_of.ensure(ss->n);
+            ss->first_col.ensure(ss->npl);
             ss->coef.ensure((size_t)ss->nleaves * 11);
             ss->fnew.ensure(ss->n);
             // reduced grid of the lattice: unique x (strictly increasing, as
@@ -510,12 +724,11 @@ struct Sim {
         for (auto& s : sp) {
             const int a = s->start;
             ProfScope prof("remesh", st);
-            k_panel_fit<<<blocks(s->nleaves), 128, 0, st>>>(s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a,
+            k_panel_fit<<<blocks(s->nleaves, 128), 128, 0, st>>>(s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a,
                                                             f.p + a, s->coef.p);
             MeshView M;
             M.rec = s->rec.p;
             M.leaf_slot = s->leaf_slot.p;
-            M.cell_leaf = s->cell_leaf.p;
             M.lat_x = s->lat_x.p;
             M.lat_p = s->lat_p.p;
             M.coef = s->coef.p;
@@ -528,13 +741,23 @@ struct Sim {
             M.dxp = L / s->npx;
             M.dpp = (s->mesh.pmax - s->mesh.pmin) / s->npp;
             M.f_beyond = s->f_beyond;
-            M.shear_t = t - t_reset;
-            k_locate_eval<<<blocks(s->n), 128, 0, st>>>(M, x.p + a, p.p + a, s->fnew.p, status.p);
+            k_shift<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, L, x.p + a, p.p + a, s->sx.p,
+                                                 status.p);
+            const size_t smem = (size_t)s->pow2 * (sizeof(double) + sizeof(int));
+            if (smem > 48 * 1024)
+                FS_CUDA(cudaFuncSetAttribute(k_row_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_row_sort<<<s->npl, 512, smem, st>>>(s->nxl, s->pow2, s->row_pts.p, s->sx.p, s->lat_p.p, s->sortx.p,
+                                                  s->sortp.p, s->order.p);
+            k_walk_first_column<<<1, 32, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
+                                                  s->first_col.p, s->leaf_of.p, status.p);
+            k_walk_rows<<<blocks(s->npl, 64), 64, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
+                                                           s->sortp.p, s->first_col.p, s->leaf_of.p, status.p);
+            k_eval_points<<<blocks(s->n), kT, 0, st>>>(M, s->sortx.p, s->sortp.p, s->order.p, s->leaf_of.p,
+                                                       s->fnew.p);
             k_reset_points<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
                                                        p.p + a, f.p + a, qw.p + a);
         }
-        FS_LAUNCHED(3LL * (long long)sp.size());
-        t_reset = t;
+        FS_LAUNCHED(7LL * (long long)sp.size());
         reduced_field();
     }
 

@@ -94,9 +94,12 @@ def test_empty_and_disjoint_sets():
 
 
 def test_uniform_lattice_field_vanishes():
-    """A uniform charge lattice has E = 0 at its points by symmetry."""
+    """A uniform charge lattice has E = 0 at its points by symmetry; the FP32
+    kernel's residue is bounded relative to the field scale sum|q|/2 = 0.5."""
     L = 2 * np.pi
     x = np.arange(4096) * (L / 4096)
     q = np.full(4096, 1.0 / 4096)
     e = M.E_MQ_DirectSum_B200(L, 0.05, "fp32c").evaluate(x, x, q)
-    assert np.max(np.abs(e)) < 1e-9
+    assert np.max(np.abs(e)) < 1e-8 * 0.5
+    e64 = M.E_MQ_DirectSum_B200(L, 0.05, "fp64").evaluate(x, x, q)
+    assert np.max(np.abs(e64)) < 1e-13
