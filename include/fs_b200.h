@@ -78,6 +78,22 @@ fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_ta
                                const double* d_sources, const double* d_q_ws, int ns,
                                void* stream);
 
+/* Allocation-free self-field: E at each of n points from the same n points
+ * (targets == sources, the simulation's use), FP32-compensated like
+ * FS_FIELD_DIRECT32C, on device pointers, synchronous on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream).
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory at call time (a pool or arena that owns the device, hosts that
+ * allocate only at start-up, threads where cudaMalloc's device-wide
+ * synchronisation is not allowed).  All scratch lives in one static device
+ * array of about 9 MiB that each GPU loading the library keeps until exit;
+ * n is limited to 32768 (larger n returns FS_ERR_ARG).  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) for that
+ * device; make that first call before any stream capture.  Calls share the
+ * array, so calls that overlap on one GPU race: serialise them. */
+fs_status fs_field_eval_noalloc(double L, double epsilon, double* d_es, const double* d_x,
+                                const double* d_q_ws, int n, void* stream);
+
 /* ------------------------------------------------------------------ session */
 /* One species of the deck (AMRSimulation_load.cpp:188-270 keys). */
 typedef struct fs_species_params {

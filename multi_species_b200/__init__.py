@@ -35,7 +35,7 @@ STATUS = {0: "FS_OK", 1: "FS_ERR_ARG", 2: "FS_ERR_CUDA", 3: "FS_ERR_NOMEM", 4: "
           9: "FS_ERR_TREE"}
 
 # Every symbol include/fs_b200.h declares (checked by the tests).
-EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
+EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device", "fs_field_eval_noalloc",
            "fs_sim_create", "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export",
            "fs_sim_import_xp", "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes",
            "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
@@ -85,6 +85,8 @@ def lib():
         L.fs_field_eval.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
         L.fs_field_eval_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                            C.c_int, C.c_void_p]
+        L.fs_field_eval_noalloc.argtypes = [C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                            C.c_void_p]
         L.fs_sim_create.argtypes = [C.POINTER(SimParams), C.POINTER(C.c_void_p)]
         L.fs_sim_destroy.argtypes = [C.c_void_p]
         L.fs_sim_step.argtypes = [C.c_void_p, C.c_int]
@@ -101,7 +103,8 @@ def lib():
         L.fs_mesh_sizes.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
         L.fs_mesh_fill.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_int, _dp, _dp, _ip, _ip, _dp]
-        for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device", "fs_sim_create",
+        for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
+                  "fs_field_eval_noalloc", "fs_sim_create",
                   "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export", "fs_sim_import_xp",
                   "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes", "fs_mesh_fill",
                   "fs_profile_enable", "fs_profile_read", "fs_profile_reset"):
@@ -208,6 +211,13 @@ class E_MQ_Treecode_B200(_Field):
                  device=0):
         kind = {"fp64": FS_FIELD_TREECODE64, "fp32c": FS_FIELD_TREECODE32C}[precision]
         super().__init__(L, epsilon, kind, mac, degree, max_source, max_target, device=device)
+
+
+def field_eval_noalloc(L, epsilon, d_es, d_x, d_q_ws, n, stream=None):
+    """fs_field_eval_noalloc: self-field of n <= 32768 points on device pointers
+    (integers), with all scratch in the library's static device array -- for
+    callers that cannot allocate device memory at call time."""
+    _check(lib().fs_field_eval_noalloc(float(L), float(epsilon), d_es, d_x, d_q_ws, int(n), stream))
 
 
 # --------------------------------------------------------------------- simulation

@@ -38,6 +38,8 @@
 // RK4 stage epilogue.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "fs_device.cuh"
 
 namespace fsb {
@@ -487,4 +489,166 @@ class Direct32c final : public FieldEngine {
 
 FieldEngine* make_direct32c(double L, double eps) { return new Direct32c(L, eps); }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the FP32-compensated self-field.
+//
+// Some callers cannot allocate device memory when they need the field: code
+// running inside a memory pool or arena that owns the whole device, embedded
+// or real-time hosts whose allocation happens once at start-up, and hosts that
+// forbid cudaMalloc/cudaFree on their calling thread because those calls
+// synchronise the device.  This variant keeps all of its scratch (sort keys,
+// tile records, prefix sums, per-target bands, chunk partials, the sort's
+// temporary storage, the timeout flag) in one file-scope device array, so a
+// call allocates nothing.  The array's size is fixed (kNoAllocBytes, about
+// 9 MiB) and every GPU that loads this library holds it until the process
+// exits; it bounds the problem size to kNoAllocMaxPoints points.
+//
+// The array is shared by every call on a device and keeps the previous call's
+// contents: everything a call reads is written by that call first, and the
+// timeout flag is cleared at the start of each call.  Calls whose work overlaps
+// on the same GPU (different streams or threads) race on the array; serialise
+// them.
+constexpr int kNoAllocMaxPoints = 32768;
+constexpr int kNoAllocMaxChunks = 16;
+constexpr size_t kNoAllocCubBytes = size_t(2) << 20;
+
+namespace {
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct NoAllocLayout {
+    size_t kin, kout, iin, iout, src2, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
+};
+
+constexpr NoAllocLayout noalloc_layout() {
+    NoAllocLayout L{};
+    size_t o = 0;
+    const size_t n = kNoAllocMaxPoints;
+    L.kin = o;     o += align256(n * sizeof(uint64_t));
+    L.kout = o;    o += align256(n * sizeof(uint64_t));
+    L.iin = o;     o += align256(n * sizeof(int));
+    L.iout = o;    o += align256(n * sizeof(int));
+    L.src2 = o;    o += align256(n * sizeof(float2));
+    L.tbase = o;   o += align256((n / kS) * sizeof(double));
+    L.qs = o;      o += align256(n * sizeof(double));
+    L.qx = o;      o += align256(n * sizeof(double));
+    L.pq = o;      o += align256(n * sizeof(double));
+    L.qxsum = o;   o += align256(sizeof(double));
+    L.info = o;    o += align256(n * sizeof(TargetInfo));
+    L.partial = o; o += align256((size_t)kNoAllocMaxChunks * n * sizeof(double));
+    L.err = o;     o += align256(sizeof(int));
+    L.cub = o;     o += kNoAllocCubBytes;
+    L.total = o;
+    return L;
+}
+
+constexpr NoAllocLayout kNoAlloc = noalloc_layout();
+constexpr size_t kNoAllocBytes = kNoAlloc.total;
+static_assert(kNoAllocMaxPoints % kTB == 0 && kNoAllocMaxPoints % kS == 0, "max size must fill whole blocks");
+
+// The scratch itself.  Host code must not use this symbol as an address: it
+// gets the device address from cudaGetSymbolAddress (noalloc_scratch()).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the first call on a device does this; cudaGetSymbolAddress does
+// not allocate).
+unsigned char* noalloc_scratch() {
+    int dev = 0;
+    FS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(FS_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            (void)cudaGetLastError();
+            fail(FS_ERR_CUDA, std::string("cudaGetSymbolAddress of the static scratch failed: ") +
+                                  cudaGetErrorString(e));
+        }
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, const double* d_q, int n,
+                       cudaStream_t st) {
+    if (!(L > 0) || !(eps > 0)) fail(FS_ERR_ARG, "L and epsilon must be positive");
+    if (n < 0) fail(FS_ERR_ARG, "n must be >= 0");
+    if (n > kNoAllocMaxPoints)
+        fail(FS_ERR_ARG, "fs_field_eval_noalloc: n = " + std::to_string(n) + " exceeds the static scratch limit of " +
+                             std::to_string(kNoAllocMaxPoints) + " points");
+    if (n == 0) return;
+    if (!d_es || !d_x || !d_q) fail(FS_ERR_ARG, "null device pointer");
+    unsigned char* base = noalloc_scratch();
+    auto at = [&](size_t off) { return base + off; };
+    uint64_t* kin = reinterpret_cast<uint64_t*>(at(kNoAlloc.kin));
+    uint64_t* kout = reinterpret_cast<uint64_t*>(at(kNoAlloc.kout));
+    int* iin = reinterpret_cast<int*>(at(kNoAlloc.iin));
+    int* iout = reinterpret_cast<int*>(at(kNoAlloc.iout));
+    float2* src2 = reinterpret_cast<float2*>(at(kNoAlloc.src2));
+    double* tbase = reinterpret_cast<double*>(at(kNoAlloc.tbase));
+    double* qs = reinterpret_cast<double*>(at(kNoAlloc.qs));
+    double* qx = reinterpret_cast<double*>(at(kNoAlloc.qx));
+    double* pq = reinterpret_cast<double*>(at(kNoAlloc.pq));
+    double* qxsum = reinterpret_cast<double*>(at(kNoAlloc.qxsum));
+    TargetInfo* info = reinterpret_cast<TargetInfo*>(at(kNoAlloc.info));
+    double* partial = reinterpret_cast<double*>(at(kNoAlloc.partial));
+    int* err = reinterpret_cast<int*>(at(kNoAlloc.err));
+    void* cub_tmp = at(kNoAlloc.cub);
+
+    const int ntiles = (n + kS - 1) / kS;
+    const int ns_pad = ntiles * kS;
+    const int tblocks = (n + kTB - 1) / kTB;
+    const int nt_pad = tblocks * kTB;
+    const int want = sm_count() * 8 * 4;
+    int nchunks = std::min(std::min(ntiles, kNoAllocMaxChunks), std::max(1, (want + tblocks - 1) / tblocks));
+    const int tpc = (ntiles + nchunks - 1) / nchunks;
+    nchunks = (ntiles + tpc - 1) / tpc;
+    size_t need = 0, b = 0;
+    FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, kin, kout, iin, iout, n, 0, 63));
+    need = std::max(need, b);
+    FS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, qs, pq, n));
+    need = std::max(need, b);
+    FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, qx, qxsum, n));
+    need = std::max(need, b);
+    if (need > kNoAllocCubBytes) fail(FS_ERR_UNSUPPORTED, "sort scratch larger than the static reserve");
+
+    FS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    const int T = 256;
+    k_wrap_keys<<<(n + T - 1) / T, T, 0, st>>>(d_x, n, L, kin, iin);
+    size_t tb = kNoAllocCubBytes;
+    FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, iin, iout, n, 0, 63, st));
+    k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, src2, tbase, qs, qx);
+    tb = kNoAllocCubBytes;
+    FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
+    tb = kNoAllocCubBytes;
+    FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
+    k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
+    const double e2 = eps * eps;
+    k_pairs32<<<dim3(tblocks, nchunks), kNT, 0, st>>>(src2, tbase, n, ntiles, tpc, info, nt_pad, L, (float)e2,
+                                                       (float)(e2 / 2), (float)(e2 * e2 / 8),
+                                                       (float)(e2 * e2 * e2 / 16), partial, err);
+    Stage S;
+    S.kind = STAGE_STORE;
+    S.out = d_es;
+    const double cbg = 1 / std::sqrt(L * L + 4 * eps * eps);
+    k_finalize32<<<(n + T - 1) / T, T, 0, st>>>(partial, nchunks, nt_pad, n, info, pq, qxsum, n, L, cbg, iout, S);
+    FS_LAUNCHED(6);
+    int h = 0;
+    FS_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FS_CUDA(cudaStreamSynchronize(st));
+    if (h) fail((fs_status)h, "device wait timed out in the field kernel");
+}
+
 }  // namespace fsb
+
+extern "C" fs_status fs_field_eval_noalloc(double L, double epsilon, double* d_es, const double* d_x,
+                                           const double* d_q_ws, int n, void* stream) {
+    return fsb::guard([&] { fsb::direct32c_noalloc(L, epsilon, d_es, d_x, d_q_ws, n, (cudaStream_t)stream); });
+}
