@@ -41,7 +41,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-MUFU_RSQ_PER_CLK_PER_SM = 16
+MUFU_PER_CLK_PER_SM = 16          # MUFU (rsqrt / rcp) lanes per clock per SM
+FP32_LANES_PER_CLK_PER_SM = 128    # FP32 FMA-pipe lanes per clock per SM
+# FP32 lane-operations per far pair in k_pairs32 (FADD2, FFMA2, FMUL2, FFMA2,
+# FFMA2 over two targets = 10, plus one FMUL for the shared reciprocal = 11 per
+# two pairs); its MUFU use is 0.5 per pair, so the FP32 datapath is the bound.
+PAIR32_FP32_OPS = 5.5
 
 
 def parse():
@@ -269,19 +274,26 @@ def run_ours(a, rank, world, local_rank):
         sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
         clocks = clk.summary()
         mhz = float(peaks.get("sm_max_mhz", 1965.0))
-        peak = sm * MUFU_RSQ_PER_CLK_PER_SM * mhz * 1e6
+        clk = mhz * 1e6
+        mufu_peak = sm * MUFU_PER_CLK_PER_SM * clk        # one MUFU op per pair
+        fp32_peak = sm * FP32_LANES_PER_CLK_PER_SM * clk / PAIR32_FP32_OPS
         achieved = kwork / (kms / 1e3) if kms > 0 else 0.0
         tr = traffic_per_pair(kern)
-        roof = {"kernel": kern, "bound": "mufu", "unit": "Gpair/s", "achieved": achieved / 1e9, "peak": peak / 1e9,
-                "frac": achieved / peak if peak else None,
-                "peak_source": f"{sm} SMs x {MUFU_RSQ_PER_CLK_PER_SM} MUFU rsqrt/clk x sm_max_mhz {mhz:.0f} "
-                               f"({peak_src} MEASURED_PEAKS.json clock); one rsqrt per pair",
+        roof = {"kernel": kern, "bound": "fp32-pipe", "unit": "Gpair/s", "achieved": achieved / 1e9,
+                "peak": fp32_peak / 1e9, "frac": achieved / fp32_peak,
+                "peak_source": f"{sm} SMs x {FP32_LANES_PER_CLK_PER_SM} FP32 lanes/clk x sm_max_mhz {mhz:.0f} "
+                               f"({peak_src} MEASURED_PEAKS.json clock) / {PAIR32_FP32_OPS} FP32 lane-ops per far "
+                               f"pair (packed FP32x2, one MUFU.RCP per two pairs)",
+                "mufu_convention": {"peak": mufu_peak / 1e9, "frac": achieved / mufu_peak,
+                                    "note": "one MUFU op + 8 FP32 ops per pair: min(FP32/8, MUFU) = 16 pairs/clk/SM"},
                 "launches": kl, "avg_launch_ms": kms / kl if kl else None,
                 "pairs_per_launch": kwork / kl if kl else None,
                 "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
                 "kernel_share_of_step_time": kms / total_ms if total_ms else None}
         if a.field == "direct64":
-            roof["bound"] = "fp64"
+            # two IEEE divisions + one square root + ~11 FP64 ops per pair, no MUFU shortcut
+            roof.update({"bound": "fp64-pipe", "peak": None, "frac": None,
+                         "peak_source": "FP64 pipe (reference arithmetic, bit-exact); not a speed-of-light kernel"})
         res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
                "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if a.field == "direct32c" else "f64",

@@ -16,20 +16,19 @@
 //    (sources before / after J_i take one of two images); the FP64 background
 //    term uses the same split, so both halves of the kernel agree exactly on
 //    which image a pair uses.
-//  * Per target the sources split into a far band (|d| > 12 eps) and a near
+//  * Per target the sources split into a far band (|d| > 24 eps) and a near
 //    band, by index (binary searches in FP64).  A far pair contributes
-//    sign(d) q/2 (1 - c(v)) with v = eps^2/(d^2+eps^2) <= 1/145: the sign(d) q/2
+//    sign(d) q/2 (1 - c(v)) with v = eps^2/(d^2+eps^2) <= 1/577: the sign(d) q/2
 //    part is summed exactly in FP64 from prefix sums of the FP64 charges; the
-//    pair kernel only
-//    accumulates q/2 * c(v), c = v/2 + v^2/8 + v^3/16 (series of 1-sqrt(1-v)),
-//    which is O(eps^2/d^2) and carries FP32's relative error on a small
-//    quantity.  Near-band pairs (|d| <= 12 eps, a few percent) use the full
-//    q/2 d*y with Kahan-compensated FP32 accumulation.  Every tile's partial
-//    sum is added into an FP64 accumulator.
-//  * Far pair: FSUB, FFMA, MUFU.RSQ, FMUL, FFMA, FFMA, FMUL, FFMA, the seven
-//    FP32 operations issued as packed FP32x2 instructions over two targets
-//    (Blackwell FADD2/FFMA2/FMUL2), so the MUFU pipe (16 rsqrt/clk/SM) and not
-//    the issue rate bounds the kernel, with source tiles
+//    pair kernel only accumulates q/2 * c(v), c = v/2 + v^2/8 (series of
+//    1-sqrt(1-v)), which is O(eps^2/d^2) and carries FP32's relative error on
+//    a small quantity.  Near-band pairs (|d| <= 24 eps, a few percent) use the
+//    full q/2 d*y with Kahan-compensated FP32 accumulation.  Every tile's
+//    partial sum is added into an FP64 accumulator.
+//  * Far pairs need no square root: per two targets, FADD2, FFMA2 (d, d^2+eps^2
+//    packed), one FMUL + one MUFU.RCP for both reciprocals, FMUL2, FFMA2,
+//    FMUL2, FFMA2 -- 6.5 FP32 lane-operations and 0.5 MUFU op per pair, so
+//    the FP32 datapath (128 lanes/clk/SM), not the MUFU pipe, bounds it; source tiles
 //    moved global->shared by TMA bulk copies (cp.async.bulk, no multicast)
 //    double-buffered on mbarriers.
 //
@@ -38,6 +37,7 @@
 // RK4 stage epilogue.
 #include <cub/cub.cuh>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "fs_device.cuh"
@@ -48,8 +48,8 @@ namespace {
 
 constexpr int kS = 256;          // sources per tile
 constexpr int kNT = 128;         // threads per CTA
-constexpr int kR = 4;            // targets per thread
-constexpr int kTB = kNT * kR;    // targets per CTA
+constexpr int kRMax = 8;         // largest number of targets per thread
+constexpr int kTBPad = kNT * kRMax;  // target counts are padded to a multiple of this
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -98,6 +98,12 @@ __device__ __forceinline__ float rsqrt_approx(float v) {
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
     return y;
 }
+// One MUFU.RCP: the argument is a product of two values in [eps^2, L^2/4+eps^2].
+__device__ __forceinline__ float rcp_approx(float v) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+}
 
 __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_double((long long)k); }
 
@@ -115,22 +121,26 @@ __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint6
     idx[i] = i;
 }
 
-// Sorted sources -> tile-relative FP32 records {s, q/2} (pads {0, 0}), the
-// FP64 tile bases, and the FP64 q and q*x the exact sums are formed from.
+// Sorted sources -> tile-relative FP32 records {s, q/2, q/2 a1, q/2 a2}
+// (pads all zero), the FP64 tile bases, and the FP64 q and q*x the exact sums
+// are formed from.  a1 = eps^2/2, a2 = eps^4/8 are the far-pair series
+// coefficients, folded into the source's charge once here.
 __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
-                                 const double* __restrict__ q, int ns, int ns_pad, float2* __restrict__ src2,
-                                 double* __restrict__ tbase, double* __restrict__ qs, double* __restrict__ qx) {
+                                 const double* __restrict__ q, int ns, int ns_pad, double a1, double a2,
+                                 float4* __restrict__ src, double* __restrict__ tbase, double* __restrict__ qs,
+                                 double* __restrict__ qx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns_pad) return;
     if (j >= ns) {
-        src2[j] = make_float2(0.f, 0.f);
+        src[j] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
     const double xj = key_to_x(skeys[j]);
     const double base = key_to_x(skeys[(j / kS) * kS]);
     if (j % kS == 0) tbase[j / kS] = base;
     const double qj = q[sidx[j]];
-    src2[j] = make_float2((float)(xj - base), (float)(0.5 * qj));
+    const float qh = (float)(0.5 * qj);
+    src[j] = make_float4((float)(xj - base), qh, (float)((double)qh * a1), (float)((double)qh * a2));
     qs[j] = qj;
     qx[j] = qj * xj;
 }
@@ -207,17 +217,21 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 }
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
-// v = eps^2 y^2 <= 1/(1 + kBand^2).  The sign part is summed in FP64 (ffar);
-// the pair kernel accumulates q/2 * c with c = z (a1 + z (a2 + z a3)),
-// z = y^2, a_k the series coefficients of 1 - sqrt(1 - v) times eps^(2k):
-// truncation error 5 v^3 / 64 relative, below FP32 rounding for kBand = 12.
-constexpr double kBand = 12.0;
+// v = eps^2 w, w = 1/(d^2 + eps^2), v <= 1/(1 + kBand^2).  The sign part is
+// summed in FP64 (ffar); the pair kernel accumulates q/2 * c with
+// c = v/2 + v^2/8 = w (a1 + a2 w), a1 = eps^2/2, a2 = eps^4/8: the truncated
+// terms are below v^2/8 <= 4e-7 of c at the band edge and fall off as 1/d^4.
+// No square root is needed for far pairs, and the reciprocals of two pairs
+// come from one MUFU.RCP of their product: w_a = r_b / (r_a r_b).
+constexpr double kBand = 24.0;
 
+template <int kR>
 __global__ void __launch_bounds__(kNT)
-k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int ns, int ntiles,
+k_pairs32(const float4* __restrict__ src, const double* __restrict__ tbase, int ns, int ntiles,
           int tiles_per_chunk, const TargetInfo* __restrict__ info, int nt_pad, double L, float eps2, float a1,
-          float a2, float a3, double* __restrict__ partial, int* __restrict__ err) {
-    __shared__ __align__(128) float2 buf[2][kS];
+          float a2, double* __restrict__ partial, int* __restrict__ err) {
+    constexpr int kTB = kNT * kR;
+    __shared__ __align__(128) float4 buf[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
     const int tid = threadIdx.x;
     const int t0 = blockIdx.y * tiles_per_chunk;
@@ -241,10 +255,10 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
         fence_mbar_init();
     }
     __syncthreads();
-    constexpr uint32_t kBytes = kS * sizeof(float2);
+    constexpr uint32_t kBytes = kS * sizeof(float4);
     if (tid == 0) {
         mbar_expect_tx(&bar[0], kBytes);
-        bulk_load(buf[0], src2 + (size_t)t0 * kS, kBytes, &bar[0]);
+        bulk_load(buf[0], src + (size_t)t0 * kS, kBytes, &bar[0]);
     }
     for (int t = t0; t < t1; ++t) {
         const int k = t - t0;
@@ -252,7 +266,7 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
         if (tid == 0 && t + 1 < t1) {
             fence_proxy_async();
             mbar_expect_tx(&bar[b ^ 1], kBytes);
-            bulk_load(buf[b ^ 1], src2 + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
+            bulk_load(buf[b ^ 1], src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
         }
         const bool ok = mbar_wait_bounded(&bar[b], (uint32_t)((k >> 1) & 1));
         if (!__syncthreads_and(ok)) {
@@ -286,11 +300,11 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
             acc[r] = 0.f;
             careful |= (s == 0.f);
         }
-        const float2* tile = buf[b];
+        const float4* tile = buf[b];
         if (!__any_sync(0xffffffffu, careful)) {
-            // far tiles: accumulate q/2 * c(v), two targets per packed FP32x2 op
-            const float2 e2v = make_float2(eps2, eps2), a1v = make_float2(a1, a1);
-            const float2 a2v = make_float2(a2, a2), a3v = make_float2(a3, a3);
+            // far tiles: accumulate q/2 * c(v) = w (q/2 a1 + q/2 a2 w), two
+            // targets per packed FP32x2 op, one MUFU.RCP per two targets
+            const float2 e2v = make_float2(eps2, eps2);
             float2 tau2[kR / 2], acc2[kR / 2];
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
@@ -299,16 +313,16 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
             }
 #pragma unroll 4
             for (int j = 0; j < kS; ++j) {
-                const float2 e = tile[j];
-                const float2 ns = make_float2(-e.x, -e.x), qh = make_float2(e.y, e.y);
+                const float4 e = tile[j];
+                const float2 ns = make_float2(-e.x, -e.x);
+                const float2 qa1 = make_float2(e.z, e.z), qa2 = make_float2(e.w, e.w);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
                     const float2 d = __fadd2_rn(tau2[h], ns);
                     const float2 r2 = __ffma2_rn(d, d, e2v);
-                    const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                    const float2 z = __fmul2_rn(y, y);
-                    const float2 p = __ffma2_rn(z, __ffma2_rn(z, a3v, a2v), a1v);
-                    acc2[h] = __ffma2_rn(qh, __fmul2_rn(z, p), acc2[h]);
+                    const float W = rcp_approx(r2.x * r2.y);
+                    const float2 w = __fmul2_rn(make_float2(r2.y, r2.x), make_float2(W, W));
+                    acc2[h] = __ffma2_rn(w, __ffma2_rn(w, qa2, qa1), acc2[h]);
                 }
             }
 #pragma unroll
@@ -323,7 +337,7 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
 #pragma unroll
             for (int r = 0; r < kR; ++r) cmp[r] = 0.f;
             for (int j = 0; j < kS; ++j) {
-                const float2 e = tile[j];
+                const float4 e = tile[j];
                 const int idx = jlo + j;
 #pragma unroll
                 for (int r = 0; r < kR; ++r) {
@@ -332,7 +346,7 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
                     const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
                     const float y = rsqrt_approx(fmaf(d, d, eps2));
                     const float z = y * y;
-                    const float c = z * fmaf(z, fmaf(z, a3, a2), a1);
+                    const float c = z * fmaf(z, a2, a1);
                     const float val = (u < U1[r]) ? -c : ((u >= U2[r]) ? c : d * y);
                     const float v = fmaf(e.y, val, -cmp[r]);
                     const float sum = acc[r] + v;
@@ -348,6 +362,18 @@ k_pairs32(const float2* __restrict__ src2, const double* __restrict__ tbase, int
     double* out = partial + (size_t)blockIdx.y * nt_pad;
 #pragma unroll
     for (int r = 0; r < kR; ++r) out[ibase + r * kNT] = acc64[r];
+}
+
+// Targets per thread of the pair kernel: 2, 4 or 8 (register use vs. reuse of
+// each shared-memory source record).
+void launch_pairs(int R, dim3 grid, cudaStream_t st, const float4* src, const double* tbase, int ns, int ntiles,
+                  int tpc, const TargetInfo* info, int nt_pad, double L, float eps2, float a1, float a2,
+                  double* partial, int* err) {
+    switch (R) {
+        case 2: k_pairs32<2><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
+        case 8: k_pairs32<8><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
+        default: k_pairs32<4><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
+    }
 }
 
 // Sum the chunk partials in a fixed order, add the exact far-band sign sum,
@@ -374,7 +400,14 @@ __global__ void k_finalize32(const double* __restrict__ partial, int nchunks, in
 
 class Direct32c final : public FieldEngine {
    public:
-    Direct32c(double L, double eps) : L_(L), eps_(eps) { cbg_ = 1 / std::sqrt(L * L + 4 * eps * eps); }
+    Direct32c(double L, double eps) : L_(L), eps_(eps) {
+        cbg_ = 1 / std::sqrt(L * L + 4 * eps * eps);
+        // tuning knob: targets per thread of the pair kernel (2, 4 or 8)
+        if (const char* v = std::getenv("FS_B200_PAIR_TARGETS")) {
+            const int r = std::atoi(v);
+            if (r == 2 || r == 4 || r == 8) R_ = r;
+        }
+    }
 
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
               cudaStream_t st) override {
@@ -383,8 +416,8 @@ class Direct32c final : public FieldEngine {
         const bool same = (d_t == d_s) && (nt == ns);
         const int ntiles = (ns + kS - 1) / kS;
         const int ns_pad = ntiles * kS;
-        const int tblocks = (nt + kTB - 1) / kTB;
-        const int nt_pad = tblocks * kTB;
+        const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
+        const int tblocks = nt_pad / (kNT * R_);
         const int sms = sm_count();
         // enough CTAs for several waves at ~8 resident CTAs per SM
         const int want = sms * 8 * 4;
@@ -399,8 +432,9 @@ class Direct32c final : public FieldEngine {
             k_wrap_keys<<<(ns + T - 1) / T, T, 0, st>>>(d_s, ns, L_, kin_.p, iin_.p);
             size_t tb = cub_.bytes();
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
-            k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, src2_.p,
-                                                                 tbase_.p, qs_.p, qx_.p);
+            const double e2 = eps_ * eps_;
+            k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
+                                                                 e2 * e2 / 8, src_.p, tbase_.p, qs_.p, qx_.p);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
             tb = cub_.bytes();
@@ -424,9 +458,8 @@ class Direct32c final : public FieldEngine {
             dim3 grid(tblocks, nchunks);
             const double e2 = eps_ * eps_;
             ProfScope prof("k_pairs32", st, last_pairs);
-            k_pairs32<<<grid, kNT, 0, st>>>(src2_.p, tbase_.p, ns, ntiles, tpc, info_.p, nt_pad, L_, (float)e2,
-                                             (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(e2 * e2 * e2 / 16),
-                                             partial_.p, err_.p);
+            launch_pairs(R_, grid, st, src_.p, tbase_.p, ns, ntiles, tpc, info_.p, nt_pad, L_, (float)e2,
+                         (float)(e2 / 2), (float)(e2 * e2 / 8), partial_.p, err_.p);
             FS_LAUNCHED(2);
         } else {
             FS_CUDA(cudaMemsetAsync(partial_.p, 0, sizeof(double) * nt_pad, st));
@@ -445,7 +478,7 @@ class Direct32c final : public FieldEngine {
         kout_.ensure(ns);
         iin_.ensure(ns);
         iout_.ensure(ns);
-        src2_.ensure(ns_pad);
+        src_.ensure(ns_pad);
         qs_.ensure(ns);
         qx_.ensure(ns);
         pq_.ensure(ns);
@@ -476,9 +509,10 @@ class Direct32c final : public FieldEngine {
     }
 
     double L_, eps_, cbg_;
+    int R_ = 4;
     DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
     DevBuf<int> iin_, iout_, tiin_, tiout_;
-    DevBuf<float2> src2_;
+    DevBuf<float4> src_;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_;
@@ -517,7 +551,7 @@ namespace {
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct NoAllocLayout {
-    size_t kin, kout, iin, iout, src2, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
+    size_t kin, kout, iin, iout, src, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
 };
 
 constexpr NoAllocLayout noalloc_layout() {
@@ -528,7 +562,7 @@ constexpr NoAllocLayout noalloc_layout() {
     L.kout = o;    o += align256(n * sizeof(uint64_t));
     L.iin = o;     o += align256(n * sizeof(int));
     L.iout = o;    o += align256(n * sizeof(int));
-    L.src2 = o;    o += align256(n * sizeof(float2));
+    L.src = o;     o += align256(n * sizeof(float4));
     L.tbase = o;   o += align256((n / kS) * sizeof(double));
     L.qs = o;      o += align256(n * sizeof(double));
     L.qx = o;      o += align256(n * sizeof(double));
@@ -544,7 +578,7 @@ constexpr NoAllocLayout noalloc_layout() {
 
 constexpr NoAllocLayout kNoAlloc = noalloc_layout();
 constexpr size_t kNoAllocBytes = kNoAlloc.total;
-static_assert(kNoAllocMaxPoints % kTB == 0 && kNoAllocMaxPoints % kS == 0, "max size must fill whole blocks");
+static_assert(kNoAllocMaxPoints % kTBPad == 0 && kNoAllocMaxPoints % kS == 0, "max size must fill whole blocks");
 
 // The scratch itself.  Host code must not use this symbol as an address: it
 // gets the device address from cudaGetSymbolAddress (noalloc_scratch()).
@@ -591,7 +625,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     uint64_t* kout = reinterpret_cast<uint64_t*>(at(kNoAlloc.kout));
     int* iin = reinterpret_cast<int*>(at(kNoAlloc.iin));
     int* iout = reinterpret_cast<int*>(at(kNoAlloc.iout));
-    float2* src2 = reinterpret_cast<float2*>(at(kNoAlloc.src2));
+    float4* src = reinterpret_cast<float4*>(at(kNoAlloc.src));
     double* tbase = reinterpret_cast<double*>(at(kNoAlloc.tbase));
     double* qs = reinterpret_cast<double*>(at(kNoAlloc.qs));
     double* qx = reinterpret_cast<double*>(at(kNoAlloc.qx));
@@ -604,8 +638,9 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
 
     const int ntiles = (n + kS - 1) / kS;
     const int ns_pad = ntiles * kS;
-    const int tblocks = (n + kTB - 1) / kTB;
-    const int nt_pad = tblocks * kTB;
+    constexpr int R = 4;
+    const int nt_pad = (n + kTBPad - 1) / kTBPad * kTBPad;
+    const int tblocks = nt_pad / (kNT * R);
     const int want = sm_count() * 8 * 4;
     int nchunks = std::min(std::min(ntiles, kNoAllocMaxChunks), std::max(1, (want + tblocks - 1) / tblocks));
     const int tpc = (ntiles + nchunks - 1) / nchunks;
@@ -624,16 +659,16 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     k_wrap_keys<<<(n + T - 1) / T, T, 0, st>>>(d_x, n, L, kin, iin);
     size_t tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, iin, iout, n, 0, 63, st));
-    k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, src2, tbase, qs, qx);
+    const double e2 = eps * eps;
+    k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, tbase,
+                                                         qs, qx);
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
-    const double e2 = eps * eps;
-    k_pairs32<<<dim3(tblocks, nchunks), kNT, 0, st>>>(src2, tbase, n, ntiles, tpc, info, nt_pad, L, (float)e2,
-                                                       (float)(e2 / 2), (float)(e2 * e2 / 8),
-                                                       (float)(e2 * e2 * e2 / 16), partial, err);
+    launch_pairs(R, dim3(tblocks, nchunks), st, src, tbase, n, ntiles, tpc, info, nt_pad, L, (float)e2,
+                 (float)(e2 / 2), (float)(e2 * e2 / 8), partial, err);
     Stage S;
     S.kind = STAGE_STORE;
     S.out = d_es;
