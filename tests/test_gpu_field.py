@@ -103,3 +103,44 @@ def test_uniform_lattice_field_vanishes():
     assert np.max(np.abs(e)) < 1e-8 * 0.5
     e64 = M.E_MQ_DirectSum_B200(L, 0.05, "fp64").evaluate(x, x, q)
     assert np.max(np.abs(e64)) < 1e-13
+
+
+# ------------------------------------------------------------------ treecode
+def test_treecode64_reference_golden():
+    g = np.load(os.path.join(GOLD, "field_treecode.npz"))
+    f = M.E_MQ_Treecode_B200(float(g["L"]), float(g["eps"]), float(g["mac"]), int(g["degree"]),
+                             int(g["max_source"]), precision="fp64")
+    e = f.evaluate(g["sources"], g["sources"], g["q"])
+    assert rel_l2(e, g["es"]) < 1e-12
+
+
+@pytest.mark.parametrize("n,leaf,mac,deg", [(1, 2000, 0.7, 8), (50, 2000, 0.7, 8), (3000, 200, 0.7, 8),
+                                            (20000, 500, 0.5, 6), (40000, 2000, 0.7, 8)])
+def test_treecode64_vs_oracle(n, leaf, mac, deg):
+    rng = np.random.default_rng(n + leaf)
+    L = 20 * np.pi
+    x = rng.uniform(-L / 2, 1.5 * L, n)
+    q = rng.normal(size=n) * 1e-4
+    ref = O.treecode(L, 0.02, mac, deg, leaf, x, q)
+    e = M.E_MQ_Treecode_B200(L, 0.02, mac, deg, leaf, precision="fp64").evaluate(x, x, q)
+    if n == 1:
+        assert np.array_equal(e, ref)
+    else:
+        assert rel_l2(e, ref) < 1e-12
+
+
+@pytest.mark.parametrize("n,leaf", [(3000, 200), (40000, 2000)])
+def test_treecode32c_vs_oracle(n, leaf):
+    rng = np.random.default_rng(7 * n)
+    L = 20 * np.pi
+    x = rng.uniform(-L / 2, 1.5 * L, n)
+    q = -np.abs(rng.normal(size=n)) * (L / n)
+    ref = O.treecode(L, 0.02, 0.7, 8, leaf, x, q)
+    e = M.E_MQ_Treecode_B200(L, 0.02, 0.7, 8, leaf, precision="fp32c").evaluate(x, x, q)
+    assert rel_l2(e, ref) < TOL32
+
+
+def test_treecode_rejects_distinct_targets():
+    f = M.E_MQ_Treecode_B200(1.0, 0.1, 0.7, 8, 100)
+    with pytest.raises(M.FsError):
+        f.evaluate(np.zeros(3), np.zeros(4), np.zeros(4))

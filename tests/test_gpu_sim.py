@@ -95,3 +95,29 @@ def test_pair_count_and_launches():
     assert M.kernel_launches() > n0
     n = g.n
     assert g.pair_count() > 4 * n * n
+
+
+def test_treecode_simulation_matches_oracle():
+    """Bump-on-tail at reduced size (3 species, 33 x 65 points each, leaf 300):
+    device treecode session vs the oracle's treecode session."""
+    d = decks.bump_on_tail(h=4, ph=1)
+    d["max_source"] = 300
+    g, o = M.Simulation(d, "treecode64"), O.Sim(d)
+    a, b = g.state(), o.state()
+    assert rel(a["es"], b["es"]) < 1e-12
+    for _ in range(5):
+        g.step()
+        o.step()
+    a, b = g.state(), o.state()
+    for k in ("xs", "ps"):
+        assert rel(a[k], b[k]) < 1e-11, k
+    assert rel(a["fs"], b["fs"]) < 1e-9
+    assert rel(a["es"], b["es"]) < 1e-9
+
+
+def test_treecode32c_simulation_field_error():
+    d = decks.bump_on_tail(h=5, ph=1)
+    g64, g32 = M.Simulation(d, "treecode64"), M.Simulation(d, "treecode32c")
+    g64.step(2)
+    g32.step(2)
+    assert rel(g32.state()["es"], g64.state()["es"]) < 1e-6
