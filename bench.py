@@ -55,8 +55,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="two_stream", choices=["two_stream", "landau"])
-    ap.add_argument("--field", default="direct32c", choices=["direct32c", "direct64"])
+    ap.add_argument("--workload", default="two_stream", choices=["two_stream", "landau", "bump_on_tail"])
+    ap.add_argument("--field", default=None, choices=["direct32c", "direct64", "treecode32c", "treecode64"],
+                    help="default: direct32c, treecode32c for bump_on_tail")
     ap.add_argument("--h", type=int, default=None, help="override the mesh height (small cases for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -69,6 +70,9 @@ def workload_deck(a):
     if a.workload == "two_stream":
         d = decks.two_stream(h=a.h or 8, ph=1, steps=100, remesh_period=5)
         name = "two_stream_precision_form"
+    elif a.workload == "bump_on_tail":
+        d = decks.bump_on_tail(h=a.h or 9, ph=1, steps=50)
+        name = "bump_on_tail_treecode"
     else:
         d = decks.landau_two_species(h=a.h or 5, ph=1)
         name = "landau_two_species"
@@ -144,17 +148,38 @@ def traffic_per_pair(kernel: str):
     return None
 
 
-def cpu_baseline(deck, seconds: float):
-    """Reference E_MQ_DirectSum on all host cores over a sample of targets."""
-    import oracle as O
+def _lattice(deck, h_drop=0):
+    """All species' mesh points and weights of a deck (optionally h reduced)."""
     import multi_species_b200 as M
-    sp = deck["species_list"][0]
-    m = M.mesh(sp["initial_height"], sp["p_height"], deck["xmin"], deck["xmax"], sp["pmin"], sp["pmax"],
-               q=sp["q"], quadrature=deck["quadrature"])
-    x = m["xs"] + 0.2 * m["ps"]
-    q = m["base_weights"]
+    xs, qs = [], []
+    for sp in deck["species_list"]:
+        m = M.mesh(max(1, sp["initial_height"] - h_drop), sp["p_height"], deck["xmin"], deck["xmax"], sp["pmin"],
+                   sp["pmax"], q=sp["q"], quadrature=deck["quadrature"])
+        xs.append(m["xs"] + 0.2 * m["ps"])
+        qs.append(m["base_weights"])
+    return np.concatenate(xs), np.concatenate(qs)
+
+
+def cpu_baseline(deck, seconds: float, treecode: bool = False):
+    """The reference's own field code (oracle/_ref) on the host cores: the
+    OpenMP direct sum over a sample of targets, or for treecode decks the
+    reference treecode (serial as shipped) on a reduced copy of the deck."""
+    import oracle as O
     L = deck["xmax"] - deck["xmin"]
     cores = os.cpu_count() or 1
+    if treecode:
+        for drop in (4, 3, 2):
+            x, q = _lattice(deck, drop)
+            t0 = time.perf_counter()
+            O.ref_treecode(L, deck["greens_epsilon"], deck["mac"], deck["degree"], deck["max_source"], x, q)
+            dt = time.perf_counter() - t0
+            if dt > seconds / 4:
+                break
+        return {"value": len(x) ** 2 / dt, "unit": "pair-interactions/s (direct-equivalent)", "cores": 1,
+                "kind": "reference",
+                "sample": f"reference E_MQ_Treecode (serial far/near loops as shipped) on the deck with mesh height "
+                          f"reduced by {drop}: {len(x)} points, one evaluation ({dt:.1f} s)"}
+    x, q = _lattice(deck)
     nt = 256
     while True:
         t0 = time.perf_counter()
@@ -179,10 +204,11 @@ def run_reference(a, rank, world):
         return None
     vals = []
     per = max(1.0, a.cpu_seconds / max(1, a.steps + a.warmup))
+    tree = int(deck.get("use_treecode", 0)) > 0
     for _ in range(a.warmup):
-        cpu_baseline(deck, per)
+        cpu_baseline(deck, per, tree)
     for _ in range(a.steps):
-        vals.append(cpu_baseline(deck, per))
+        vals.append(cpu_baseline(deck, per, tree))
     v = statistics.median(x["value"] for x in vals)
     cb = dict(vals[-1])
     cb["value"] = v
@@ -195,9 +221,115 @@ def run_reference(a, rank, world):
             "e2e": {"value": v, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+KERNEL_OF_FIELD = {"direct32c": "k_pairs32", "direct64": "k_direct64", "treecode32c": "k_near32",
+                   "treecode64": "k_far_near64"}
+
+
+def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
+    """Roofline object for the dominant kernel of the field kind."""
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    clk_hz = mhz * 1e6
+    mufu_peak = sm * MUFU_PER_CLK_PER_SM * clk_hz        # one MUFU op per pair
+    fp32_peak = sm * FP32_LANES_PER_CLK_PER_SM * clk_hz / PAIR32_FP32_OPS
+    achieved = kwork / (kms / 1e3) if kms > 0 else 0.0
+    tr = traffic_per_pair(kern)
+    roof = {"kernel": kern, "bound": "fp32-pipe", "unit": "Gpair/s", "achieved": achieved / 1e9,
+            "peak": fp32_peak / 1e9, "frac": achieved / fp32_peak,
+            "peak_source": f"{sm} SMs x {FP32_LANES_PER_CLK_PER_SM} FP32 lanes/clk x sm_max_mhz {mhz:.0f} "
+                           f"({peak_src} MEASURED_PEAKS.json clock) / {PAIR32_FP32_OPS} FP32 lane-ops per far "
+                           f"pair (packed FP32x2, one MUFU.RCP per two pairs)",
+            "mufu_convention": {"peak": mufu_peak / 1e9, "frac": achieved / mufu_peak,
+                                "note": "one MUFU op + 8 FP32 ops per pair: min(FP32/8, MUFU) = 16 pairs/clk/SM"},
+            "launches": kl, "avg_launch_ms": kms / kl if kl else None,
+            "pairs_per_launch": kwork / kl if kl else None,
+            "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
+            "kernel_share_of_step_time": kms / total_ms if total_ms else None}
+    if a.field == "direct64":
+        # two IEEE divisions + one square root + ~11 FP64 ops per pair, no MUFU shortcut
+        roof.update({"bound": "fp64-pipe", "peak": None, "frac": None, "mufu_convention": None,
+                     "peak_source": "FP64 pipe (reference arithmetic, bit-exact); not a speed-of-light kernel"})
+    elif a.field.startswith("treecode"):
+        roof.update({"bound": "mufu", "peak": mufu_peak / 1e9, "unit": "Gpair/s (direct-equivalent)",
+                     "frac": None, "mufu_convention": None,
+                     "peak_source": "near-field pairs need one MUFU rsqrt each (16/clk/SM)",
+                     "note": "achieved is direct-equivalent N^2 pairs per near-kernel time; see kernel_evals_per_s"})
+    return roof
+
+
+def run_ours(a, rank, world, local_rank):
+    import multi_species_b200 as M
+    import torch
+    name, deck = workload_deck(a)
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    sim = M.Simulation(deck, field_backend=a.field, device=local_rank)
+    n = sim.n
+    for _ in range(a.warmup):
+        sim.step(1)
+    M.profile_reset()
+    M.profile_enable(True)
+    launches0 = M.kernel_launches()
+    pairs0, evals0 = sim.work()
+    step_ms = []
+    dist = world > 1
+    if dist:
+        import torch.distributed as D
+        D.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sim.step(1)
+            step_ms.extend(sim.step_times().tolist())
+    torch.cuda.synchronize()
+    if dist:
+        D.barrier()
+    M.profile_enable(False)
+    launches = M.kernel_launches() - launches0
+    pairs1, evals1 = sim.work()
+    pairs, evals = pairs1 - pairs0, evals1 - evals0
+    total_ms = float(np.sum(step_ms))
+    kern = KERNEL_OF_FIELD[a.field]
+    kl, kms, kwork = M.profile_read(kern)
+    rl, rms, _ = M.profile_read("remesh")
+    t_max = total_ms
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        t_max = float(t.item())
+        pw = torch.tensor([pairs, evals], dtype=torch.float64)
+        D.all_reduce(pw, op=D.ReduceOp.SUM)
+        pairs, evals = float(pw[0].item()), float(pw[1].item())
+    value = pairs / (t_max / 1e3)
+    res = None
+    if rank == 0:
+        peaks, peak_src = measured_peaks()
+        sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+        res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
+               "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if a.field.endswith("32c") else "f64",
+               "data": "synthetic (deck-generated, no dataset)",
+               "config": {"workload": name, "points": n, "field": a.field, "eps": deck["greens_epsilon"],
+                          "dt": deck["dt"], "remesh_period": deck["remesh_period"], "parallelism": f"replicas{world}",
+                          "l2": "flushed (256 MiB write) between timed steps"},
+               "rk4_steps_per_s": a.steps / (t_max / 1e3) * world,
+               "kernel_evals_per_s": evals / (t_max / 1e3),
+               "remesh_ms_per_remesh": (rms / rl) if rl else None,
+               "gpu_launches": int(launches),
+               "roofline": roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src),
+               "clocks": clk.summary()}
+        if not a.no_e2e:
+            res["e2e"] = e2e_plugin(deck, a.field, n, local_rank)
+        if not a.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(deck, a.cpu_seconds, a.field.startswith("treecode"))
+    sim.close()
+    return res
+
+
 def host_rk4_step(field, xs, ps, es, qw, qm, dt):
     """AMRSimulation::rk4_step + end-of-step field on the host, each field
-    evaluation through the plugin call with host arrays."""
+    evaluation through the plugin call with host arrays (qm per point)."""
     n = len(xs)
     ef1 = es * qm
     p2 = ps + 0.5 * dt * ef1
@@ -222,106 +354,20 @@ def host_rk4_step(field, xs, ps, es, qw, qm, dt):
     return xs, ps, es
 
 
-def run_ours(a, rank, world, local_rank):
-    import multi_species_b200 as M
-    import torch
-    name, deck = workload_deck(a)
-    torch.cuda.set_device(local_rank)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
-    sim = M.Simulation(deck, field_backend=a.field, device=local_rank)
-    n = sim.n
-    for _ in range(a.warmup):
-        sim.step(1)
-    M.profile_reset()
-    M.profile_enable(True)
-    launches0 = M.kernel_launches()
-    pairs0 = sim.pair_count()
-    step_ms = []
-    dist = world > 1
-    if dist:
-        import torch.distributed as D
-        D.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local_rank) as clk:
-        for _ in range(a.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            sim.step(1)
-            step_ms.extend(sim.step_times().tolist())
-    torch.cuda.synchronize()
-    if dist:
-        D.barrier()
-    M.profile_enable(False)
-    launches = M.kernel_launches() - launches0
-    pairs = sim.pair_count() - pairs0
-    total_ms = float(np.sum(step_ms))
-    kern = "k_pairs32" if a.field == "direct32c" else "k_direct64"
-    kl, kms, kwork = M.profile_read(kern)
-    rl, rms, _ = M.profile_read("remesh")
-    t_max = total_ms
-    pairs_all = pairs
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        t_max = float(t.item())
-        pw = torch.tensor([pairs], dtype=torch.float64)
-        D.all_reduce(pw, op=D.ReduceOp.SUM)
-        pairs_all = float(pw.item())
-    value = pairs_all / (t_max / 1e3)
-    res = None
-    if rank == 0:
-        peaks, peak_src = measured_peaks()
-        sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
-        clocks = clk.summary()
-        mhz = float(peaks.get("sm_max_mhz", 1965.0))
-        clk = mhz * 1e6
-        mufu_peak = sm * MUFU_PER_CLK_PER_SM * clk        # one MUFU op per pair
-        fp32_peak = sm * FP32_LANES_PER_CLK_PER_SM * clk / PAIR32_FP32_OPS
-        achieved = kwork / (kms / 1e3) if kms > 0 else 0.0
-        tr = traffic_per_pair(kern)
-        roof = {"kernel": kern, "bound": "fp32-pipe", "unit": "Gpair/s", "achieved": achieved / 1e9,
-                "peak": fp32_peak / 1e9, "frac": achieved / fp32_peak,
-                "peak_source": f"{sm} SMs x {FP32_LANES_PER_CLK_PER_SM} FP32 lanes/clk x sm_max_mhz {mhz:.0f} "
-                               f"({peak_src} MEASURED_PEAKS.json clock) / {PAIR32_FP32_OPS} FP32 lane-ops per far "
-                               f"pair (packed FP32x2, one MUFU.RCP per two pairs)",
-                "mufu_convention": {"peak": mufu_peak / 1e9, "frac": achieved / mufu_peak,
-                                    "note": "one MUFU op + 8 FP32 ops per pair: min(FP32/8, MUFU) = 16 pairs/clk/SM"},
-                "launches": kl, "avg_launch_ms": kms / kl if kl else None,
-                "pairs_per_launch": kwork / kl if kl else None,
-                "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
-                "kernel_share_of_step_time": kms / total_ms if total_ms else None}
-        if a.field == "direct64":
-            # two IEEE divisions + one square root + ~11 FP64 ops per pair, no MUFU shortcut
-            roof.update({"bound": "fp64-pipe", "peak": None, "frac": None,
-                         "peak_source": "FP64 pipe (reference arithmetic, bit-exact); not a speed-of-light kernel"})
-        res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
-               "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if a.field == "direct32c" else "f64",
-               "data": "synthetic (deck-generated, no dataset)",
-               "config": {"workload": name, "points": n, "field": a.field, "eps": deck["greens_epsilon"],
-                          "dt": deck["dt"], "remesh_period": deck["remesh_period"], "parallelism": f"replicas{world}",
-                          "l2": "flushed (256 MiB write) between timed steps"},
-               "rk4_steps_per_s": a.steps / (t_max / 1e3) * world,
-               "remesh_ms_per_remesh": (rms / rl) if rl else None,
-               "gpu_launches": int(launches), "roofline": roof, "clocks": clocks}
-        if not a.no_e2e:
-            res["e2e"] = e2e_plugin(deck, a.field, n, local_rank)
-        if not a.no_cpu_baseline:
-            res["cpu_baseline"] = cpu_baseline(deck, a.cpu_seconds)
-    sim.close()
-    return res
-
-
 def e2e_plugin(deck, field_kind, n, device):
     import multi_species_b200 as M
     sim = M.Simulation(deck, field_backend=field_kind, device=device)
     st = sim.state()
+    counts = sim.species_points
     sim.close()
     L = deck["xmax"] - deck["xmin"]
-    f = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], "fp32c" if field_kind == "direct32c" else "fp64",
-                              device=device)
-    sp = deck["species_list"][0]
-    qm = sp["q"] / sp["m"]
+    prec = "fp32c" if field_kind.endswith("32c") else "fp64"
+    if field_kind.startswith("treecode"):
+        f = M.E_MQ_Treecode_B200(L, deck["greens_epsilon"], deck["mac"], deck["degree"], deck["max_source"],
+                                 precision=prec, device=device)
+    else:
+        f = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], prec, device=device)
+    qm = np.concatenate([np.full(c, sp["q"] / sp["m"]) for c, sp in zip(counts, deck["species_list"])])
     xs, ps, es, qw = st["xs"], st["ps"], st["es"], st["q_ws"]
     xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"])  # warm-up
     steps = 2
@@ -333,11 +379,13 @@ def e2e_plugin(deck, field_kind, n, device):
     pairs = 4.0 * n * n * steps
     return {"value": pairs / dt, "unit": "pair-interactions/s", "h2d_bytes_per_step": 4 * 16 * n,
             "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
-            "path": "E_MQ_DirectSum_B200(es, targets, nt, sources, q_ws, ns) with host arrays, host RK4"}
+            "path": f"{type(f).__name__}(es, targets, nt, sources, q_ws, ns) with host arrays, host RK4"}
 
 
 def main():
     a = parse()
+    if a.field is None:
+        a.field = "treecode32c" if a.workload == "bump_on_tail" else "direct32c"
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

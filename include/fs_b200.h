@@ -145,6 +145,10 @@ fs_status fs_sim_import_xp(fs_sim* sim, const double* xs, const double* ps, cons
 fs_status fs_sim_iter(const fs_sim* sim, int* iter, double* t);
 /* Pair interactions evaluated so far (full + reduced), for throughput metrics. */
 fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs);
+/* Direct-equivalent pairs (N^2 per evaluation) and kernel-level evaluations
+ * (treecode: near pairs + far cluster terms; counted while profiling is
+ * enabled, otherwise equal to the direct-equivalent count). */
+fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_evals);
 
 /* ------------------------------------------------------------- host mesh */
 /* Sizes of the uniform periodic panel mesh of create_prerefined_mesh. */

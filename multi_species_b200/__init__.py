@@ -37,7 +37,7 @@ STATUS = {0: "FS_OK", 1: "FS_ERR_ARG", 2: "FS_ERR_CUDA", 3: "FS_ERR_NOMEM", 4: "
 # Every symbol include/fs_b200.h declares (checked by the tests).
 EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device", "fs_field_eval_noalloc",
            "fs_sim_create", "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export",
-           "fs_sim_import_xp", "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes",
+           "fs_sim_import_xp", "fs_sim_iter", "fs_sim_pair_count", "fs_sim_work", "fs_sim_step_times", "fs_mesh_sizes",
            "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
            "fs_version", "fs_kernel_launches"]
 
@@ -97,6 +97,7 @@ def lib():
         L.fs_sim_iter.argtypes = [C.c_void_p, _ip, _dp]
         L.fs_sim_pair_count.argtypes = [C.c_void_p, _dp]
         L.fs_sim_step_times.argtypes = [C.c_void_p, _dp, C.c_int, _ip]
+        L.fs_sim_work.argtypes = [C.c_void_p, _dp, _dp]
         L.fs_profile_enable.argtypes = [C.c_int]
         L.fs_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), _dp, _dp]
         L.fs_profile_reset.argtypes = []
@@ -106,7 +107,8 @@ def lib():
         for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
                   "fs_field_eval_noalloc", "fs_sim_create",
                   "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export", "fs_sim_import_xp",
-                  "fs_sim_iter", "fs_sim_pair_count", "fs_sim_step_times", "fs_mesh_sizes", "fs_mesh_fill",
+                  "fs_sim_iter", "fs_sim_pair_count", "fs_sim_work", "fs_sim_step_times", "fs_mesh_sizes",
+                  "fs_mesh_fill",
                   "fs_profile_enable", "fs_profile_read", "fs_profile_reset"):
             getattr(L, n).restype = st
         L.fs_last_error.restype = C.c_char_p
@@ -296,6 +298,12 @@ class Simulation:
         i, t = C.c_int(), C.c_double()
         _check(lib().fs_sim_iter(self._h, C.byref(i), C.byref(t)))
         return i.value, t.value
+
+    def work(self):
+        """(direct-equivalent pairs, kernel-level evaluations) so far."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().fs_sim_work(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def step_times(self):
         """Device ms of each step of the last step() call (CUDA events on the sim stream)."""

@@ -138,6 +138,13 @@ class FieldEngine {
                       int ns, const Stage& stage, cudaStream_t st) = 0;
     // Device int set non-zero by a kernel whose bounded wait gave up (or null).
     virtual int* error_flag() { return nullptr; }
+    // Kernel-level evaluations of the last call (pairs for the direct sums;
+    // near pairs + far cluster terms for the treecode).  May synchronise `st`;
+    // called only when profiling is enabled.
+    virtual double actual_work(cudaStream_t st) {
+        (void)st;
+        return last_pairs;
+    }
     // Pair interactions (direct-equivalent) of the last call.
     double last_pairs = 0;
 };

@@ -511,7 +511,7 @@ struct SpeciesState {
 struct Sim {
     fs_sim_params prm{};
     int N = 0, U = 0, iter = 0;
-    double L = 0, t = 0, pairs = 0;
+    double L = 0, t = 0, pairs = 0, evals = 0;
     std::vector<std::unique_ptr<SpeciesState>> sp;
     DevBuf<double> x, p, f, qw, e, xkA, xkB, pst, accX, accP, rx, rw, re;
     DevBuf<int> status;
@@ -696,6 +696,12 @@ struct Sim {
         check_status();
     }
 
+    // direct-equivalent pairs always; kernel-level evaluations when profiling
+    void account() {
+        pairs += field->last_pairs;
+        evals += profiling_enabled() ? field->actual_work(st) : field->last_pairs;
+    }
+
     Stage stage(int kind, double* xk_out) const {
         Stage S = base;
         S.kind = kind;
@@ -713,7 +719,7 @@ struct Sim {
         S.kind = STAGE_STORE;
         S.out = re.p;
         field->eval(rx.p, U, rx.p, rw.p, U, S, st);
-        pairs += field->last_pairs;
+        account();
         for (auto& s : sp) {
             k_scatter_reduced<<<blocks(s->n), kT, 0, st>>>(s->n, s->inv.p, re.p, e.p + s->start);
         }
@@ -768,11 +774,11 @@ struct Sim {
         k_rk_stage1<<<blocks(N), kT, 0, st>>>(N, S1, e.p, xkA.p);
         FS_LAUNCHED(1);
         field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK2, xkB.p), st);
-        pairs += field->last_pairs;
+        account();
         field->eval(xkB.p, N, xkB.p, qw.p, N, stage(STAGE_RK3, xkA.p), st);
-        pairs += field->last_pairs;
+        account();
         field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK4, nullptr), st);
-        pairs += field->last_pairs;
+        account();
         iter += 1;
         t += prm.dt;
         if (iter % prm.remesh_period == 0) {
@@ -782,7 +788,7 @@ struct Sim {
             S.kind = STAGE_STORE;
             S.out = e.p;
             field->eval(x.p, N, x.p, qw.p, N, S, st);
-            pairs += field->last_pairs;
+            account();
         }
     }
 
@@ -906,6 +912,14 @@ fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs) {
     return fsb::guard([&] {
         if (!sim || !pairs) fsb::fail(FS_ERR_ARG, "null argument");
         *pairs = sim->impl.pairs;
+    });
+}
+
+fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_evals) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null argument");
+        if (direct_pairs) *direct_pairs = sim->impl.pairs;
+        if (kernel_evals) *kernel_evals = sim->impl.evals;
     });
 }
 

@@ -583,6 +583,24 @@ __global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b
     if (i < n) c[i] = a[i] * b[i];
 }
 
+// near pairs + far cluster terms of this call
+__global__ void k_count_work(const TNode* __restrict__ nodes, const int* __restrict__ meta,
+                             const int* __restrict__ leaves, const int* __restrict__ far_n,
+                             const int* __restrict__ near_list, const int* __restrict__ near_n, int P,
+                             double* __restrict__ work) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= meta[1] || meta[2]) return;
+    const TNode lf = nodes[leaves[l]];
+    const double nt = lf.m1 - lf.m0 + 1;
+    double ns = 0.0;
+    for (int q = 0; q < near_n[l]; ++q) {
+        const TNode nd = nodes[near_list[(size_t)l * kNearCap + q]];
+        ns += nd.m1 - nd.m0 + 1;
+    }
+    atomicAdd(&work[0], nt * ns);
+    atomicAdd(&work[1], nt * far_n[l] * (double)(P + 1));
+}
+
 __global__ void k_copy_meta_error(const int* __restrict__ meta, int* __restrict__ err) {
     if (meta[2]) atomicCAS(err, 0, meta[2]);
 }
@@ -611,6 +629,18 @@ class Treecode final : public FieldEngine {
 
     int* error_flag() override { return err_.p; }
 
+    double actual_work(cudaStream_t st) override {
+        if (last_pairs <= 0) return 0.0;
+        FS_CUDA(cudaMemsetAsync(work_.p, 0, 2 * sizeof(double), st));
+        k_count_work<<<(cap_leaves_ + 127) / 128, 128, 0, st>>>(nodes_.p, meta_.p, leaves_.p, far_n_.p, near_.p,
+                                                                near_n_.p, P_, work_.p);
+        FS_LAUNCHED(1);
+        double h[2] = {0, 0};
+        FS_CUDA(cudaMemcpyAsync(h, work_.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+        FS_CUDA(cudaStreamSynchronize(st));
+        return h[0] + h[1];
+    }
+
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
               cudaStream_t st) override {
         (void)d_t;
@@ -622,6 +652,7 @@ class Treecode final : public FieldEngine {
         const int cap_nodes = 2 * kMaxDepth * (n / N0_ + 1) + 64;
         const int cap_items = cap_nodes + (int)(((long long)n * (kMaxDepth + 1)) / kChunk) + 1;
         reserve(n, cap_nodes, cap_leaves, cap_items);
+        cap_leaves_ = cap_leaves;
         const int T = 256;
         k_tree_keys<<<(n + T - 1) / T, T, 0, st>>>(d_s, n, L_, kin_.p, iin_.p);
         size_t tb = cub_.bytes();
@@ -685,6 +716,7 @@ class Treecode final : public FieldEngine {
         nodes_.ensure(cap_nodes);
         leaves_.ensure(cap_leaves);
         meta_.ensure(4);
+        work_.ensure(2);
         far_.ensure((size_t)cap_leaves * kFarCap);
         far_n_.ensure(cap_leaves);
         near_.ensure((size_t)cap_leaves * kNearCap);
@@ -714,7 +746,8 @@ class Treecode final : public FieldEngine {
     double norm_ = 1, cbg_ = 0;
     DevBuf<uint64_t> kin_, kout_;
     DevBuf<int> iin_, iout_, leaf_of_, leaves_, meta_, far_, far_n_, near_, near_n_, counts_, item_start_, err_;
-    DevBuf<double> sx_, lam_, efar_, mpart_, mom_, consts_, pl_, plx_, lx_;
+    DevBuf<double> sx_, lam_, efar_, mpart_, mom_, consts_, pl_, plx_, lx_, work_;
+    int cap_leaves_ = 0;
     DevBuf<TNode> nodes_;
     DevBuf<unsigned char> cub_;
 };
