@@ -55,7 +55,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="two_stream", choices=["two_stream", "landau", "bump_on_tail"])
+    ap.add_argument("--workload", default="two_stream",
+                    choices=["two_stream", "landau", "bump_on_tail", "landau_batch"])
+    ap.add_argument("--batch", type=int, default=64, help="instances of the landau_batch workload")
     ap.add_argument("--field", default=None, choices=["direct32c", "direct64", "treecode32c", "treecode64"],
                     help="default: direct32c, treecode32c for bump_on_tail")
     ap.add_argument("--h", type=int, default=None, help="override the mesh height (small cases for profiling)")
@@ -73,6 +75,11 @@ def workload_deck(a):
     elif a.workload == "bump_on_tail":
         d = decks.bump_on_tail(h=a.h or 9, ph=1, steps=50)
         name = "bump_on_tail_treecode"
+    elif a.workload == "landau_batch":
+        # the batch's largest instance stands in for it where one deck is needed
+        ds = decks.landau_batch(count=a.batch, seed=0)
+        d = max(ds, key=decks.deck_points)
+        name = f"landau_batch{a.batch}"
     else:
         d = decks.landau_two_species(h=a.h or 5, ph=1)
         name = "landau_two_species"
@@ -327,6 +334,96 @@ def run_ours(a, rank, world, local_rank):
     return res
 
 
+def run_batch(a, rank, world, local_rank):
+    """landau_batch: independent Landau instances of 2k-200k points stepped
+    together (fs_batch_*: one persistent pair launch per field evaluation,
+    autotuned items, graph-replayed steps).  Next to it, the plain FP64 GPU
+    path (direct64, one simulation at a time) on the batch's largest instance."""
+    import multi_species_b200 as M
+    import torch
+    from multi_species_b200 import decks
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+    ds = decks.landau_batch(count=a.batch, seed=0)
+    b = M.Batch(device=local_rank)
+    ids = [b.add(d) for d in ds]
+    npts = [b.info(i)["n"] for i in ids]
+    for _ in range(a.warmup):
+        b.step(1)
+    M.profile_reset()
+    M.profile_enable(True)
+    launches0 = M.kernel_launches()
+    pairs0 = b.pair_count()
+    step_ms = []
+    dist = world > 1
+    if dist:
+        import torch.distributed as D
+        D.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        for _ in range(a.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            b.step(1)
+            step_ms.extend(b.step_times().tolist())
+    torch.cuda.synchronize()
+    if dist:
+        D.barrier()
+    M.profile_enable(False)
+    launches = M.kernel_launches() - launches0
+    pairs = b.pair_count() - pairs0
+    kl, kms, kwork = M.profile_read("k_pairs32_batched")
+    stats = b.stats()
+    b.close()
+    total_ms = float(np.sum(step_ms))
+    t_max = total_ms
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64)
+        D.all_reduce(t, op=D.ReduceOp.MAX)
+        t_max = float(t.item())
+        pw = torch.tensor([pairs], dtype=torch.float64)
+        D.all_reduce(pw, op=D.ReduceOp.SUM)
+        pairs = float(pw[0].item())
+    value = pairs / (t_max / 1e3)
+    if rank != 0:
+        return None
+    # plain FP64 GPU path on the largest instance, same device
+    big = max(ds, key=decks.deck_points)
+    sim = M.Simulation(big, field_backend="direct64", device=local_rank)
+    sim.step(1)
+    w0, _ = sim.work()
+    sim.step(2)
+    w1, _ = sim.work()
+    plain = (w1 - w0) / (float(np.sum(sim.step_times())) / 1e3)
+    sim.close()
+    peaks, peak_src = measured_peaks()
+    sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    a.field = "direct32c"
+    roof = roofline(a, "k_pairs32_batched", kl, kms, kwork, total_ms, sm, peaks, peak_src)
+    res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (deck-generated, no dataset)",
+           "config": {"workload": f"landau_batch{a.batch}", "instances": len(ds), "points_total": int(sum(npts)),
+                      "points_min": int(min(npts)), "points_max": int(max(npts)), "field": "direct32c",
+                      "eps": 0.05, "dt": 0.25, "remesh_period": 5, "parallelism": f"replicas{world}",
+                      "l2": "flushed (256 MiB write) between timed steps",
+                      "tuning": {k: stats[k] for k in ("targets_per_thread", "tiles_per_item")},
+                      "graph_steps": stats["graph_steps"], "plain_steps": stats["plain_steps"]},
+           "rk4_steps_per_s": a.steps * len(ds) / (t_max / 1e3) * world,
+           "plain_fp64_gpu": {"value": plain, "unit": "pair-interactions/s",
+                              "path": "direct64 Simulation (reference arithmetic), largest instance alone",
+                              "points": decks.deck_points(big)},
+           "speedup_vs_plain_fp64_gpu": value / plain,
+           "step_ms_p50": float(np.percentile(step_ms, 50)), "step_ms_p99": float(np.percentile(step_ms, 99)),
+           "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
+    if not a.no_e2e:
+        res["e2e"] = e2e_plugin(big, "direct32c", decks.deck_points(big), local_rank)
+        res["e2e"]["note"] = "plugin path on the batch's largest instance"
+    if not a.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_baseline(big, a.cpu_seconds, False)
+    return res
+
+
 def host_rk4_step(field, xs, ps, es, qw, qm, dt):
     """AMRSimulation::rk4_step + end-of-step field on the host, each field
     evaluation through the plugin call with host arrays (qm per point)."""
@@ -397,6 +494,8 @@ def main():
     try:
         if a.impl == "reference":
             res = run_reference(a, rank, world)
+        elif a.workload == "landau_batch":
+            res = run_batch(a, rank, world, local_rank)
         else:
             res = run_ours(a, rank, world, local_rank)
         if rank == 0 and res is not None:

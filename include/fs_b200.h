@@ -150,6 +150,46 @@ fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs);
  * enabled, otherwise equal to the direct-equivalent count). */
 fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_evals);
 
+/* ------------------------------------------------------------------ batch */
+/* Many independent simulations stepped together on one device and stream
+ * (no counterpart in the reference, which runs one deck per process).  Each
+ * of a step's four field evaluations runs every member's preparation, then
+ * the FP32 pair work of all FS_FIELD_DIRECT32C members as one persistent
+ * launch over work items taken longest first; other kinds evaluate on their
+ * own in the same stream.  Results equal those of fs_sim_step on each member
+ * alone (the pair sums are made in the same fixed order).  The first step
+ * times the candidate item shapes and keeps the fastest; later steps of
+ * all-direct batches are captured once per remesh pattern into a CUDA graph
+ * and replayed.  Adding or removing a member discards the graphs. */
+typedef struct fs_batch fs_batch;
+
+fs_status fs_batch_create(int device, fs_batch** out);
+fs_status fs_batch_destroy(fs_batch* batch);
+/* Create a member (as fs_sim_create; params->device must be the batch's). */
+fs_status fs_batch_add(fs_batch* batch, const fs_sim_params* params, int* id);
+fs_status fs_batch_remove(fs_batch* batch, int id);
+/* nsteps steps of every member, synchronous on return. */
+fs_status fs_batch_step(fs_batch* batch, int nsteps);
+/* As fs_sim_export for member `id`. */
+fs_status fs_batch_export(fs_batch* batch, int id, double* xs, double* ps, double* fs, double* q_ws, double* es);
+/* Points, steps taken, time and pair interactions of member `id` (NULL to skip). */
+fs_status fs_batch_info(fs_batch* batch, int id, int* npoints, int* iter, double* t, double* pairs);
+/* Device time of each step of the last fs_batch_step call, ms. */
+fs_status fs_batch_step_times(fs_batch* batch, double* ms, int cap, int* n);
+/* Pair interactions of all members so far. */
+fs_status fs_batch_work(fs_batch* batch, double* pairs);
+/* Chosen item shape (targets per thread, source tiles of 256 per item) and
+ * the number of steps replayed from graphs / run launch by launch. */
+fs_status fs_batch_stats(fs_batch* batch, int* targets_per_thread, int* tiles_per_item, long long* graph_steps,
+                         long long* plain_steps);
+/* Fix the item shape instead of autotuning (targets per thread 4 or 8, source
+ * tiles per item >= 1).  Pair sums are then made in the same order whatever
+ * the other members are, so a member's results are bit-identical alone and in
+ * any mix. */
+fs_status fs_batch_set_tuning(fs_batch* batch, int targets_per_thread, int tiles_per_item);
+/* Graph capture on (default) or off; either way discards existing graphs. */
+fs_status fs_batch_set_graphs(fs_batch* batch, int on);
+
 /* ------------------------------------------------------------- host mesh */
 /* Sizes of the uniform periodic panel mesh of create_prerefined_mesh. */
 fs_status fs_mesh_sizes(int initial_height, int p_height, int* npoints, int* npanels, int* nleaves);

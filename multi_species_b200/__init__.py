@@ -39,7 +39,9 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_sim_create", "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export",
            "fs_sim_import_xp", "fs_sim_iter", "fs_sim_pair_count", "fs_sim_work", "fs_sim_step_times", "fs_mesh_sizes",
            "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
-           "fs_version", "fs_kernel_launches"]
+           "fs_version", "fs_kernel_launches", "fs_batch_create", "fs_batch_destroy", "fs_batch_add",
+           "fs_batch_remove", "fs_batch_step", "fs_batch_export", "fs_batch_info", "fs_batch_step_times",
+           "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs"]
 
 
 class FsError(RuntimeError):
@@ -104,6 +106,22 @@ def lib():
         L.fs_mesh_sizes.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
         L.fs_mesh_fill.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                    C.c_int, _dp, _dp, _ip, _ip, _dp]
+        L.fs_batch_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        L.fs_batch_destroy.argtypes = [C.c_void_p]
+        L.fs_batch_add.argtypes = [C.c_void_p, C.POINTER(SimParams), _ip]
+        L.fs_batch_remove.argtypes = [C.c_void_p, C.c_int]
+        L.fs_batch_step.argtypes = [C.c_void_p, C.c_int]
+        L.fs_batch_export.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.fs_batch_info.argtypes = [C.c_void_p, C.c_int, _ip, _ip, _dp, _dp]
+        L.fs_batch_step_times.argtypes = [C.c_void_p, _dp, C.c_int, _ip]
+        L.fs_batch_work.argtypes = [C.c_void_p, _dp]
+        L.fs_batch_stats.argtypes = [C.c_void_p, _ip, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.fs_batch_set_graphs.argtypes = [C.c_void_p, C.c_int]
+        L.fs_batch_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        for n in ("fs_batch_create", "fs_batch_destroy", "fs_batch_add", "fs_batch_remove", "fs_batch_step",
+                  "fs_batch_export", "fs_batch_info", "fs_batch_step_times", "fs_batch_work", "fs_batch_stats",
+                  "fs_batch_set_tuning", "fs_batch_set_graphs"):
+            getattr(L, n).restype = st
         for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
                   "fs_field_eval_noalloc", "fs_sim_create",
                   "fs_sim_destroy", "fs_sim_step", "fs_sim_remesh", "fs_sim_num_points", "fs_sim_export", "fs_sim_import_xp",
@@ -332,6 +350,84 @@ class Simulation:
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().fs_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------- batch
+class Batch:
+    """Many independent simulations stepped together on one GPU (fs_batch_*).
+
+    Members are decks as for Simulation; their FP32 pair work shares one
+    persistent launch per field evaluation, and steps are replayed from CUDA
+    graphs once captured.  No counterpart in the reference (one deck per run).
+    """
+
+    def __init__(self, device: int = 0, graphs: bool = True, tuning=None):
+        h = C.c_void_p()
+        _check(lib().fs_batch_create(int(device), C.byref(h)))
+        self._h = h
+        self.device = int(device)
+        self.members = {}
+        if not graphs:
+            _check(lib().fs_batch_set_graphs(self._h, 0))
+        if tuning is not None:
+            self.set_tuning(*tuning)
+
+    def set_tuning(self, targets_per_thread: int, tiles_per_item: int) -> None:
+        """Fix the item shape (skips the autotuner)."""
+        _check(lib().fs_batch_set_tuning(self._h, int(targets_per_thread), int(tiles_per_item)))
+
+    def add(self, deck: dict, field_backend: str | None = None) -> int:
+        p = sim_params(deck, field_backend, self.device)
+        i = C.c_int()
+        _check(lib().fs_batch_add(self._h, C.byref(p), C.byref(i)))
+        self.members[i.value] = deck
+        return i.value
+
+    def remove(self, sim_id: int) -> None:
+        _check(lib().fs_batch_remove(self._h, int(sim_id)))
+        self.members.pop(sim_id, None)
+
+    def step(self, n: int = 1) -> None:
+        _check(lib().fs_batch_step(self._h, int(n)))
+
+    def info(self, sim_id: int) -> dict:
+        n, it, t, w = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+        _check(lib().fs_batch_info(self._h, int(sim_id), C.byref(n), C.byref(it), C.byref(t), C.byref(w)))
+        return {"n": n.value, "iter": it.value, "t": t.value, "pairs": w.value}
+
+    def state(self, sim_id: int) -> dict:
+        n = self.info(sim_id)["n"]
+        a = {k: np.zeros(n) for k in ("xs", "ps", "fs", "q_ws", "es")}
+        _check(lib().fs_batch_export(self._h, int(sim_id), *(_ptr(a[k]) for k in ("xs", "ps", "fs", "q_ws", "es"))))
+        return a
+
+    def step_times(self):
+        buf = np.zeros(4096)
+        n = C.c_int()
+        _check(lib().fs_batch_step_times(self._h, _ptr(buf), len(buf), C.byref(n)))
+        return buf[: n.value].copy()
+
+    def pair_count(self) -> float:
+        v = C.c_double()
+        _check(lib().fs_batch_work(self._h, C.byref(v)))
+        return v.value
+
+    def stats(self) -> dict:
+        r, t, g, pl = C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong()
+        _check(lib().fs_batch_stats(self._h, C.byref(r), C.byref(t), C.byref(g), C.byref(pl)))
+        return {"targets_per_thread": r.value, "tiles_per_item": t.value, "graph_steps": g.value,
+                "plain_steps": pl.value}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fs_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -167,13 +167,6 @@ __device__ __forceinline__ double unrolled_prefix(const double* __restrict__ inc
     return k * incl[n - 1] + (r ? incl[r - 1] : 0.0);
 }
 
-struct TargetInfo {
-    double tlo;   // target coordinate for sources before J (after J: tlo + L)
-    double ffar;  // exact FP64 sum of sign(d) * q/2 over the far band (FP64 q)
-    int J, U1, U2;
-    int pad;
-};
-
 // Per sorted target: the image split J, the near band [U1, U2) in unrolled
 // index space (|d| <= band), and the far-band sign sum.
 __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt_pad,
@@ -225,59 +218,57 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // come from one MUFU.RCP of their product: w_a = r_b / (r_a r_b).
 constexpr double kBand = 24.0;
 
+// One (target block, source chunk) of a job: kR targets per thread, the
+// chunk's tiles moved into shared memory by TMA bulk copies on two mbarriers.
+// `gk` counts the tiles this CTA has consumed (buffer = gk & 1, barrier phase
+// = (gk >> 1) & 1), so the barriers keep alternating across work items.
+// Returns false when a bounded wait gave up (flag set, CTA must stop).
 template <int kR>
-__global__ void __launch_bounds__(kNT)
-k_pairs32(const float4* __restrict__ src, const double* __restrict__ tbase, int ns, int ntiles,
-          int tiles_per_chunk, const TargetInfo* __restrict__ info, int nt_pad, double L, float eps2, float a1,
-          float a2, double* __restrict__ partial, int* __restrict__ err) {
+__device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk, float4 (*buf)[kS], uint64_t* bar,
+                                           uint32_t& gk, int* __restrict__ err) {
     constexpr int kTB = kNT * kR;
-    __shared__ __align__(128) float4 buf[2][kS];
-    __shared__ __align__(8) uint64_t bar[2];
     const int tid = threadIdx.x;
-    const int t0 = blockIdx.y * tiles_per_chunk;
-    const int t1 = min(ntiles, t0 + tiles_per_chunk);
-    if (t0 >= t1) return;
-    const int ibase = blockIdx.x * kTB + tid;
+    const int t0 = chunk * Jb.tpc;
+    const int t1 = min(Jb.ntiles, t0 + Jb.tpc);
+    if (t0 >= t1) return true;
+    const float eps2 = Jb.eps2, a1 = Jb.a1, a2 = Jb.a2;
+    const double L = Jb.L;
+    const int ns = Jb.ns;
+    const int ibase = tb * kTB + tid;
     double tl[kR], acc64[kR];
     int J[kR], U1[kR], U2[kR];
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-        const TargetInfo T = info[ibase + r * kNT];  // nt_pad is a multiple of kTB
+        const TargetInfo T = Jb.info[ibase + r * kNT];  // nt_pad is a multiple of kTB
         tl[r] = T.tlo;
         J[r] = T.J;
         U1[r] = T.U1;
         U2[r] = T.U2;
         acc64[r] = 0.0;
     }
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
     constexpr uint32_t kBytes = kS * sizeof(float4);
     if (tid == 0) {
-        mbar_expect_tx(&bar[0], kBytes);
-        bulk_load(buf[0], src + (size_t)t0 * kS, kBytes, &bar[0]);
+        fence_proxy_async();
+        mbar_expect_tx(&bar[gk & 1], kBytes);
+        bulk_load(buf[gk & 1], Jb.src + (size_t)t0 * kS, kBytes, &bar[gk & 1]);
     }
-    for (int t = t0; t < t1; ++t) {
-        const int k = t - t0;
-        const int b = k & 1;
+    for (int t = t0; t < t1; ++t, ++gk) {
+        const int b = gk & 1;
         if (tid == 0 && t + 1 < t1) {
             fence_proxy_async();
             mbar_expect_tx(&bar[b ^ 1], kBytes);
-            bulk_load(buf[b ^ 1], src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
+            bulk_load(buf[b ^ 1], Jb.src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
         }
-        const bool ok = mbar_wait_bounded(&bar[b], (uint32_t)((k >> 1) & 1));
+        const bool ok = mbar_wait_bounded(&bar[b], (gk >> 1) & 1);
         if (!__syncthreads_and(ok)) {
             if (tid == 0) {
                 atomicExch(err, (int)FS_ERR_TIMEOUT);
                 // let a copy still in flight land before the CTA's shared memory is released
-                if (t + 1 < t1) (void)mbar_wait_bounded(&bar[b ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+                if (t + 1 < t1) (void)mbar_wait_bounded(&bar[b ^ 1], ((gk + 1) >> 1) & 1);
             }
-            return;
+            return false;
         }
-        const double base = tbase[t];
+        const double base = Jb.tbase[t];
         const int jlo = t * kS;
         const int jend = min(jlo + kS, ns);  // real sources in this tile
         float tau[kR], tauh[kR], sg[kR], acc[kR];
@@ -287,18 +278,18 @@ k_pairs32(const float4* __restrict__ src, const double* __restrict__ tbase, int 
             const double lo = tl[r] - base;
             tau[r] = (float)lo;
             tauh[r] = (float)(lo + L);
-            float s = 0.f;
+            float sgn = 0.f;
             if (jend <= J[r]) {          // whole tile on the lo image: u = j + n
-                if (jend + ns <= U1[r]) s = 1.f;
-                else if (jlo + ns >= U2[r]) s = -1.f;
+                if (jend + ns <= U1[r]) sgn = 1.f;
+                else if (jlo + ns >= U2[r]) sgn = -1.f;
             } else if (jlo >= J[r]) {    // whole tile on the hi image: u = j
                 tau[r] = tauh[r];
-                if (jend <= U1[r]) s = 1.f;
-                else if (jlo >= U2[r]) s = -1.f;
+                if (jend <= U1[r]) sgn = 1.f;
+                else if (jlo >= U2[r]) sgn = -1.f;
             }
-            sg[r] = s;
+            sg[r] = sgn;
             acc[r] = 0.f;
-            careful |= (s == 0.f);
+            careful |= (sgn == 0.f);
         }
         const float4* tile = buf[b];
         if (!__any_sync(0xffffffffu, careful)) {
@@ -314,11 +305,11 @@ k_pairs32(const float4* __restrict__ src, const double* __restrict__ tbase, int 
 #pragma unroll 4
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
-                const float2 ns = make_float2(-e.x, -e.x);
+                const float2 nsx = make_float2(-e.x, -e.x);
                 const float2 qa1 = make_float2(e.z, e.z), qa2 = make_float2(e.w, e.w);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
-                    const float2 d = __fadd2_rn(tau2[h], ns);
+                    const float2 d = __fadd2_rn(tau2[h], nsx);
                     const float2 r2 = __ffma2_rn(d, d, e2v);
                     const float W = rcp_approx(r2.x * r2.y);
                     const float2 w = __fmul2_rn(make_float2(r2.y, r2.x), make_float2(W, W));
@@ -359,22 +350,101 @@ k_pairs32(const float4* __restrict__ src, const double* __restrict__ tbase, int 
         }
         __syncthreads();
     }
-    double* out = partial + (size_t)blockIdx.y * nt_pad;
+    double* out = Jb.partial + (size_t)chunk * Jb.nt_pad;
 #pragma unroll
     for (int r = 0; r < kR; ++r) out[ibase + r * kNT] = acc64[r];
+    return true;
+}
+
+__device__ __forceinline__ void init_bars(uint64_t* bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+// One job, grid (target blocks, source chunks).
+template <int kR>
+__global__ void __launch_bounds__(kNT) k_pairs32(PairJob job, int* __restrict__ err) {
+    __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(8) uint64_t bar[2];
+    if ((int)blockIdx.y * job.tpc >= job.ntiles) return;
+    init_bars(bar);
+    uint32_t gk = 0;
+    (void)pair_block<kR>(job, blockIdx.x, blockIdx.y, buf, bar, gk, err);
+}
+
+// Many jobs (one per simulation of a batch), persistent: a fixed grid of CTAs
+// takes (job, target block, chunk) items from an atomic counter; items are
+// ordered longest first.
+template <int kR>
+__global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items,
+                                                         int nitems, int* __restrict__ counter, int* __restrict__ err) {
+    __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_item;
+    init_bars(bar);
+    uint32_t gk = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= nitems) break;
+        const int4 it = items[item];
+        const PairJob job = jobs[it.x];
+        if (!pair_block<kR>(job, it.y, it.z, buf, bar, gk, err)) return;
+    }
 }
 
 // Targets per thread of the pair kernel: 2, 4 or 8 (register use vs. reuse of
 // each shared-memory source record).
-void launch_pairs(int R, dim3 grid, cudaStream_t st, const float4* src, const double* tbase, int ns, int ntiles,
-                  int tpc, const TargetInfo* info, int nt_pad, double L, float eps2, float a1, float a2,
-                  double* partial, int* err) {
+void launch_pairs(int R, dim3 grid, cudaStream_t st, const PairJob& job, int* err) {
     switch (R) {
-        case 2: k_pairs32<2><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
-        case 8: k_pairs32<8><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
-        default: k_pairs32<4><<<grid, kNT, 0, st>>>(src, tbase, ns, ntiles, tpc, info, nt_pad, L, eps2, a1, a2, partial, err); break;
+        case 2: k_pairs32<2><<<grid, kNT, 0, st>>>(job, err); break;
+        case 8: k_pairs32<8><<<grid, kNT, 0, st>>>(job, err); break;
+        default: k_pairs32<4><<<grid, kNT, 0, st>>>(job, err); break;
     }
 }
+
+}  // namespace
+
+void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs, const int4* items, int nitems,
+                          int* counter, int* err) {
+    FS_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+    switch (R) {
+        case 2: k_pairs32_batched<2><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
+        case 8: k_pairs32_batched<8><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
+        default: k_pairs32_batched<4><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
+    }
+    FS_LAUNCHED(1);
+}
+
+void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost) {
+    const int tblocks = job.nt_pad / (kNT * R);
+    const int nchunks = (job.ntiles + job.tpc - 1) / job.tpc;
+    for (int c = 0; c < nchunks; ++c) {
+        const int tiles = std::min(job.tpc, job.ntiles - c * job.tpc);
+        for (int b = 0; b < tblocks; ++b) {
+            items.push_back(make_int4(job_index, b, c, 0));
+            cost.push_back((double)tiles * kNT * R);
+        }
+    }
+}
+
+int pairs_batched_grid(int R) {
+    int per_sm = 0;
+    switch (R) {
+        case 2: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_batched<2>, kNT, 0)); break;
+        case 8: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_batched<8>, kNT, 0)); break;
+        default: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_batched<4>, kNT, 0)); break;
+    }
+    return std::max(1, per_sm) * sm_count();
+}
+
+namespace {
 
 // Sum the chunk partials in a fixed order, add the exact far-band sign sum,
 // subtract the FP64 background and apply the stage epilogue at the target's
@@ -411,28 +481,41 @@ class Direct32c final : public FieldEngine {
 
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
               cudaStream_t st) override {
+        // chunking for a standalone launch: enough CTAs for several waves
+        const int ntiles = (ns + kS - 1) / kS;
+        const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
+        const int tblocks = nt_pad / (kNT * R_);
+        const int want = sm_count() * 8 * 4;
+        int nchunks = ntiles ? std::min(ntiles, std::max(1, (want + tblocks - 1) / tblocks)) : 1;
+        const int tpc = ntiles ? (ntiles + nchunks - 1) / nchunks : 1;
+        PairJob job;
+        if (prepare(d_t, nt, d_s, d_q, ns, stage, st, tpc, &job)) {
+            nchunks = (job.ntiles + job.tpc - 1) / job.tpc;
+            ProfScope prof("k_pairs32", st, last_pairs);
+            launch_pairs(R_, dim3(job.nt_pad / (kNT * R_), nchunks), st, job, err_.p);
+            FS_LAUNCHED(1);
+        }
+        finalize(st);
+    }
+
+    bool prepare(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
+                 cudaStream_t st, int tpc, PairJob* job) override {
         last_pairs = (double)nt * (double)ns;
-        if (nt <= 0) return;
+        fin_ = Fin{};
+        if (nt <= 0) return false;
         const bool same = (d_t == d_s) && (nt == ns);
         const int ntiles = (ns + kS - 1) / kS;
         const int ns_pad = ntiles * kS;
         const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
-        const int tblocks = nt_pad / (kNT * R_);
-        const int sms = sm_count();
-        // enough CTAs for several waves at ~8 resident CTAs per SM
-        const int want = sms * 8 * 4;
-        int nchunks = ntiles ? std::min(ntiles, std::max(1, (want + tblocks - 1) / tblocks)) : 1;
-        const int tpc = ntiles ? (ntiles + nchunks - 1) / nchunks : 1;
-        nchunks = ntiles ? (ntiles + tpc - 1) / tpc : 1;
+        tpc = std::max(1, tpc);
+        const int nchunks = ntiles ? (ntiles + tpc - 1) / tpc : 1;
         reserve(std::max(ns, 1), ns_pad, same ? 0 : nt, nt_pad, (size_t)nchunks * nt_pad, ntiles);
         const int T = 256;
-        const uint64_t* tkeys;
-        const int* tperm;
+        const double e2 = eps_ * eps_;
         if (ns > 0) {
             k_wrap_keys<<<(ns + T - 1) / T, T, 0, st>>>(d_s, ns, L_, kin_.p, iin_.p);
             size_t tb = cub_.bytes();
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
-            const double e2 = eps_ * eps_;
             k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
                                                                  e2 * e2 / 8, src_.p, tbase_.p, qs_.p, qx_.p);
             tb = cub_.bytes();
@@ -441,6 +524,8 @@ class Direct32c final : public FieldEngine {
             FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
             FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
         }
+        const uint64_t* tkeys;
+        const int* tperm;
         if (same) {
             tkeys = kout_.p;
             tperm = iout_.p;
@@ -452,22 +537,26 @@ class Direct32c final : public FieldEngine {
             tperm = tiout_.p;
             FS_LAUNCHED(1);
         }
-        if (ns > 0) {
-            k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_,
-                                                             pq_.p, info_.p);
-            dim3 grid(tblocks, nchunks);
-            const double e2 = eps_ * eps_;
-            ProfScope prof("k_pairs32", st, last_pairs);
-            launch_pairs(R_, grid, st, src_.p, tbase_.p, ns, ntiles, tpc, info_.p, nt_pad, L_, (float)e2,
-                         (float)(e2 / 2), (float)(e2 * e2 / 8), partial_.p, err_.p);
-            FS_LAUNCHED(2);
-        } else {
+        fin_ = Fin{true, nt, ns, nt_pad, ns > 0 ? nchunks : 1, tperm, stage};
+        if (ns <= 0) {
             FS_CUDA(cudaMemsetAsync(partial_.p, 0, sizeof(double) * nt_pad, st));
-            nchunks = 1;
+            return false;
         }
-        k_finalize32<<<(nt + T - 1) / T, T, 0, st>>>(partial_.p, nchunks, nt_pad, nt, info_.p, pq_.p, qxsum_.p, ns,
-                                                      L_, cbg_, tperm, stage);
+        k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_, pq_.p,
+                                                         info_.p);
         FS_LAUNCHED(1);
+        *job = PairJob{src_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), 0};
+        return true;
+    }
+
+    void finalize(cudaStream_t st) override {
+        if (!fin_.pending) return;
+        const int T = 256;
+        k_finalize32<<<(fin_.nt + T - 1) / T, T, 0, st>>>(partial_.p, fin_.nchunks, fin_.nt_pad, fin_.nt, info_.p,
+                                                           pq_.p, qxsum_.p, fin_.ns, L_, cbg_, fin_.tperm, fin_.stage);
+        FS_LAUNCHED(1);
+        fin_.pending = false;
     }
 
     int* error_flag() override { return err_.p; }
@@ -508,8 +597,15 @@ class Direct32c final : public FieldEngine {
         cub_.ensure(need);
     }
 
+    struct Fin {
+        bool pending = false;
+        int nt = 0, ns = 0, nt_pad = 0, nchunks = 1;
+        const int* tperm = nullptr;
+        Stage stage;
+    };
     double L_, eps_, cbg_;
     int R_ = 4;
+    Fin fin_;
     DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
@@ -667,8 +763,9 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
-    launch_pairs(R, dim3(tblocks, nchunks), st, src, tbase, n, ntiles, tpc, info, nt_pad, L, (float)e2,
-                 (float)(e2 / 2), (float)(e2 * e2 / 8), partial, err);
+    const PairJob job{src, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
+                      (float)(e2 * e2 / 8), 0};
+    launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;
     S.out = d_es;

@@ -51,10 +51,32 @@ class ProfScope {
     cudaStream_t st_;
     double work_;
     cudaEvent_t a_ = nullptr, b_ = nullptr;
+    bool captured_ = false;
 };
 bool profiling_enabled();
 
+// Profiled regions inside a captured CUDA graph: while a sink is set on this
+// thread, a ProfScope on a capturing stream records its two events as graph
+// nodes (external event records) and appends them to the sink; the graph's
+// owner adds their times to the profile after each replay.
+struct ProfNode {
+    const char* name;
+    cudaEvent_t a, b;
+    double work;
+};
+void prof_capture_sink(std::vector<ProfNode>* sink);
+void prof_harvest(const std::vector<ProfNode>& nodes);  // events must have completed
+void prof_release(std::vector<ProfNode>& nodes);
+
 // ------------------------------------------------------------------ device buffers
+// Bumped by every device (re)allocation of a DevBuf; a captured CUDA graph
+// records it and is discarded when it changed, since the graph's kernels hold
+// raw device pointers.
+inline std::atomic<unsigned long long>& alloc_epoch() {
+    static std::atomic<unsigned long long> e{0};
+    return e;
+}
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
@@ -66,6 +88,7 @@ struct DevBuf {
     void ensure(size_t count) {
         if (count <= n && p) return;
         release();
+        alloc_epoch().fetch_add(1);
         size_t bytes = (count ? count : 1) * sizeof(T);
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) {
@@ -128,6 +151,26 @@ struct HostMesh {
 double f0_value(int ics_type, double pth, double pstr, double k, double amp, double x, double p);
 
 // ------------------------------------------------------------------ field engines
+// Per sorted target of the FP32 direct sum (csrc/fs_direct32.cu).
+struct TargetInfo {
+    double tlo;   // target coordinate for sources before J (after J: tlo + L)
+    double ffar;  // exact FP64 sum of sign(d) * q/2 over the far band (FP64 q)
+    int J, U1, U2;
+    int pad;
+};
+
+// One field evaluation's FP32 pair work, as the pair kernels see it.
+struct PairJob {
+    const float4* src;        // tile-relative source records {s, q/2, q/2 a1, q/2 a2}
+    const double* tbase;      // FP64 tile bases
+    const TargetInfo* info;   // per sorted target (nt_pad entries)
+    double* partial;          // chunks * nt_pad
+    int ns, ntiles, tpc, nt_pad;
+    double L;
+    float eps2, a1, a2;
+    int pad;
+};
+
 class FieldEngine {
    public:
     virtual ~FieldEngine() = default;
@@ -145,6 +188,19 @@ class FieldEngine {
         (void)st;
         return last_pairs;
     }
+    // Batched use.  prepare() runs everything before the pair kernel with
+    // `tpc` source tiles per work chunk and fills *job, returning true; the
+    // caller then runs the pair work (alone or batched with other jobs) and
+    // calls finalize().  Engines whose work cannot join a batched launch
+    // evaluate completely here and return false (no finalize).
+    virtual bool prepare(const double* d_t, int nt, const double* d_s, const double* d_q, int ns,
+                         const Stage& stage, cudaStream_t st, int tpc, PairJob* job) {
+        (void)tpc;
+        (void)job;
+        eval(d_t, nt, d_s, d_q, ns, stage, st);
+        return false;
+    }
+    virtual void finalize(cudaStream_t st) { (void)st; }
     // Pair interactions (direct-equivalent) of the last call.
     double last_pairs = 0;
 };
@@ -152,6 +208,15 @@ class FieldEngine {
 // Runs fn, converting FsError / exceptions into an fs_status and recording the
 // message for fs_last_error().
 fs_status guard(const std::function<void()>& fn);
+
+// Batched FP32 pair work (csrc/fs_direct32.cu): one persistent launch over the
+// (job, target block, source chunk) items of many field evaluations.
+void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs, const int4* items, int nitems,
+                          int* counter, int* err);
+int pairs_batched_grid(int R);
+// Items of one job for R targets per thread (target blocks x chunks) and the
+// work of each (tiles x targets), appended to `items` / `cost`.
+void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost);
 
 FieldEngine* make_direct64(double L, double eps);
 FieldEngine* make_direct32c(double L, double eps);

@@ -32,7 +32,11 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <array>
+#include <map>
 #include <memory>
+#include <set>
+#include <string>
 
 #include "fs_device.cuh"
 
@@ -521,10 +525,12 @@ struct Sim {
     std::vector<double> step_ms;
     Stage base;
 
+    bool own_stream = true;
+
     ~Sim() {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (st) cudaStreamDestroy(st);
+        if (st && own_stream) cudaStreamDestroy(st);
     }
 
     void check_status() {
@@ -545,13 +551,18 @@ struct Sim {
         }
     }
 
-    void create(const fs_sim_params& P) {
+    void create(const fs_sim_params& P, cudaStream_t external = nullptr) {
         prm = P;
         if (P.num_species < 1 || P.num_species > 8) fail(FS_ERR_ARG, "num_species must be 1..8");
         if (!(P.xmax > P.xmin)) fail(FS_ERR_ARG, "xmax must exceed xmin");
         if (P.remesh_period < 1) fail(FS_ERR_ARG, "remesh_period must be >= 1");
         FS_CUDA(cudaSetDevice(P.device));
-        FS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (external) {
+            st = external;
+            own_stream = false;
+        } else {
+            FS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        }
         FS_CUDA(cudaEventCreate(&ev0));
         FS_CUDA(cudaEventCreate(&ev1));
         L = P.xmax - P.xmin;
@@ -709,24 +720,48 @@ struct Sim {
         return S;
     }
 
-    void reduced_field() {
+    // One field evaluation: targets == sources == x (n points), weights q.
+    struct FieldCall {
+        const double* x;
+        int n;
+        const double* q;
+        Stage stage;
+    };
+
+    void run_call(const FieldCall& fc) {
+        field->eval(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, st);
+        account();
+    }
+
+    // Reduced grid (evaluate_field_uniform_grid): column sums, one field call
+    // on the unique x, scatter back to the points.
+    void reduced_pre() {
         for (auto& s : sp) {
             k_column_sums<<<blocks(s->nu), kT, 0, st>>>(s->nu, s->col_off.p, s->col_idx.p, qw.p + s->start,
                                                        rw.p + s->roff);
         }
         FS_LAUNCHED((long long)sp.size());
+    }
+    FieldCall reduced_call() const {
         Stage S = base;
         S.kind = STAGE_STORE;
         S.out = re.p;
-        field->eval(rx.p, U, rx.p, rw.p, U, S, st);
-        account();
+        return FieldCall{rx.p, U, rw.p, S};
+    }
+    void reduced_post() {
         for (auto& s : sp) {
             k_scatter_reduced<<<blocks(s->n), kT, 0, st>>>(s->n, s->inv.p, re.p, e.p + s->start);
         }
         FS_LAUNCHED((long long)sp.size());
     }
+    void reduced_field() {
+        reduced_pre();
+        run_call(reduced_call());
+        reduced_post();
+    }
 
-    void remesh() {
+    // AMRStructure::remesh for every species (interpolation + weights).
+    void remesh_kernels() {
         for (auto& s : sp) {
             const int a = s->start;
             ProfScope prof("remesh", st);
@@ -764,31 +799,62 @@ struct Sim {
                                                        p.p + a, f.p + a, qw.p + a);
         }
         FS_LAUNCHED(7LL * (long long)sp.size());
+    }
+
+    void remesh() {
+        remesh_kernels();
         reduced_field();
     }
 
+    // A step (AMRSimulation::step, AMRSimulation_step.cpp:5-99) is four field
+    // evaluations with work before and after each:
+    //   0: RK stage 1 kernel, field at xk (epilogue: stage 2)
+    //   1: field at xk (epilogue: stage 3)
+    //   2: field at xk (epilogue: final combination)
+    //   3: iter++, t += dt; either remesh + reduced-grid field, or the field
+    //      at the new positions.
+    // Stage positions alternate between two buffers so no kernel writes the
+    // positions it reads.
+    bool remeshing = false;
+
+    void pre_call(int c) {
+        if (c == 0) {
+            Stage S1 = base;
+            k_rk_stage1<<<blocks(N), kT, 0, st>>>(N, S1, e.p, xkA.p);
+            FS_LAUNCHED(1);
+        } else if (c == 3) {
+            iter += 1;
+            t += prm.dt;
+            remeshing = (iter % prm.remesh_period == 0);
+            if (remeshing) {
+                remesh_kernels();
+                reduced_pre();
+            }
+        }
+    }
+    FieldCall call(int c) const {
+        switch (c) {
+            case 0: return FieldCall{xkA.p, N, qw.p, stage(STAGE_RK2, xkB.p)};
+            case 1: return FieldCall{xkB.p, N, qw.p, stage(STAGE_RK3, xkA.p)};
+            case 2: return FieldCall{xkA.p, N, qw.p, stage(STAGE_RK4, nullptr)};
+            default: {
+                if (remeshing) return reduced_call();
+                Stage S = base;
+                S.kind = STAGE_STORE;
+                S.out = e.p;
+                return FieldCall{x.p, N, qw.p, S};
+            }
+        }
+    }
+    void post_call(int c) {
+        if (c == 3 && remeshing) reduced_post();
+    }
+
     void step() {
-        // RK4 (AMRSimulation_step.cpp:122-263); stage positions alternate
-        // between two buffers so no kernel writes the positions it reads.
-        Stage S1 = base;
-        k_rk_stage1<<<blocks(N), kT, 0, st>>>(N, S1, e.p, xkA.p);
-        FS_LAUNCHED(1);
-        field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK2, xkB.p), st);
-        account();
-        field->eval(xkB.p, N, xkB.p, qw.p, N, stage(STAGE_RK3, xkA.p), st);
-        account();
-        field->eval(xkA.p, N, xkA.p, qw.p, N, stage(STAGE_RK4, nullptr), st);
-        account();
-        iter += 1;
-        t += prm.dt;
-        if (iter % prm.remesh_period == 0) {
-            remesh();
-        } else {
-            Stage S = base;
-            S.kind = STAGE_STORE;
-            S.out = e.p;
-            field->eval(x.p, N, x.p, qw.p, N, S, st);
-            account();
+        for (int c = 0; c < 4; ++c) {
+            pre_call(c);
+            run_call(call(c));
+            post_call(c);
         }
     }
 
@@ -920,6 +986,508 @@ fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_ev
         if (!sim) fsb::fail(FS_ERR_ARG, "null argument");
         if (direct_pairs) *direct_pairs = sim->impl.pairs;
         if (kernel_evals) *kernel_evals = sim->impl.evals;
+    });
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Batch: many independent simulations stepped together.
+//
+// Members share one stream.  For each of a step's four field evaluations,
+// every member runs its own preparation (RK stage kernels, sort, tile records,
+// band searches) and then the FP32 pair work of ALL members runs as one
+// persistent launch (k_pairs32_batched) over (member, target block, source
+// chunk) items taken longest first from an atomic counter, so simulations of
+// very different sizes share the GPU without tails.  Members whose field kind
+// cannot join (FP64 reference kernel, treecode) evaluate on their own in the
+// same stream.  The first step autotunes the items (targets per thread x
+// source tiles per item) by timing the batched launch; later steps are
+// captured once into a CUDA graph per step kind (with / without remesh) and
+// replayed while all members are in phase.
+// ======================================================================
+namespace fsb {
+
+struct Batch {
+    // Device copy of one batched launch's job and item arrays, with the host
+    // bytes they were made from.
+    struct Slot {
+        DevBuf<PairJob> jobs;
+        DevBuf<int4> items;
+        std::vector<unsigned char> host;  // jobs then items, as uploaded
+        int njobs = 0, nitems = 0;
+    };
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long epoch = 0;
+        long long launches = 0;
+        std::vector<double> dpairs, devals;  // per member, per step
+        std::vector<ProfNode> prof;          // profiled regions recorded in the graph
+    };
+    struct Capturing {};  // thrown when a captured step would need a host upload
+
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<std::unique_ptr<Sim>> sims;
+    std::vector<int> ids;
+    int next_id = 1;
+    int R = 4, tpc = 32;
+    bool tuned = false;
+    DevBuf<int> counter, err;
+    // slots and graphs are keyed by the step's remesh mask (one char per member)
+    std::map<std::string, std::array<Slot, 4>> slots;
+    std::map<std::string, Graph> graphs;
+    std::set<std::string> warmed, uncapturable;
+    bool use_graphs = true;
+    bool capturing = false;
+    std::vector<double> step_ms;
+    double pairs = 0;
+    long long graph_steps = 0, plain_steps = 0;
+
+    ~Batch() {
+        reset_graphs();
+        if (st) cudaStreamSynchronize(st);
+        sims.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    void init(int dev) {
+        device = dev;
+        FS_CUDA(cudaSetDevice(dev));
+        FS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        FS_CUDA(cudaEventCreate(&ev0));
+        FS_CUDA(cudaEventCreate(&ev1));
+        counter.ensure(1);
+        err.ensure(1);
+        FS_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+    }
+
+    void reset_graphs() {
+        for (auto& kv : graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            prof_release(kv.second.prof);
+        }
+        graphs.clear();
+        warmed.clear();
+        uncapturable.clear();
+        slots.clear();
+    }
+
+    int add(const fs_sim_params& P) {
+        if (P.device != device) fail(FS_ERR_ARG, "simulation device differs from the batch device");
+        FS_CUDA(cudaStreamSynchronize(st));
+        auto s = std::make_unique<Sim>();
+        s->create(P, st);
+        sims.push_back(std::move(s));
+        ids.push_back(next_id);
+        reset_graphs();
+        return next_id++;
+    }
+
+    int index_of(int id) const {
+        for (size_t i = 0; i < ids.size(); ++i)
+            if (ids[i] == id) return (int)i;
+        fail(FS_ERR_ARG, "no simulation with id " + std::to_string(id));
+    }
+
+    void remove(int id) {
+        const int i = index_of(id);
+        FS_CUDA(cudaStreamSynchronize(st));
+        reset_graphs();
+        sims.erase(sims.begin() + i);
+        ids.erase(ids.begin() + i);
+    }
+
+    // Items of all jobs, longest first, in host bytes (jobs then items).
+    std::vector<unsigned char> pack(const std::vector<PairJob>& jobs, int R_, int& nitems) const {
+        std::vector<int4> items;
+        std::vector<double> cost;
+        for (size_t j = 0; j < jobs.size(); ++j) pair_job_items(jobs[j], (int)j, R_, items, cost);
+        std::vector<int> order(items.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        nitems = (int)items.size();
+        std::vector<unsigned char> bytes(sizeof(PairJob) * jobs.size() + sizeof(int4) * items.size());
+        std::memcpy(bytes.data(), jobs.data(), sizeof(PairJob) * jobs.size());
+        // the item block starts at 72 * jobs bytes: not 16-byte aligned for an
+        // odd job count, so copy bytewise rather than through an int4 pointer
+        unsigned char* dst = bytes.data() + sizeof(PairJob) * jobs.size();
+        for (size_t i = 0; i < order.size(); ++i) std::memcpy(dst + i * sizeof(int4), &items[order[i]], sizeof(int4));
+        return bytes;
+    }
+
+    // Bring the slot's device arrays up to date (never while capturing).
+    void stage(Slot& sl, const std::vector<PairJob>& jobs, int R_) {
+        int nitems = 0;
+        std::vector<unsigned char> bytes = pack(jobs, R_, nitems);
+        if (bytes == sl.host && sl.jobs.p) return;
+        if (capturing) throw Capturing{};
+        sl.jobs.ensure(jobs.size());
+        sl.items.ensure(std::max(nitems, 1));
+        FS_CUDA(cudaMemcpyAsync(sl.jobs.p, bytes.data(), sizeof(PairJob) * jobs.size(), cudaMemcpyHostToDevice, st));
+        FS_CUDA(cudaMemcpyAsync(sl.items.p, bytes.data() + sizeof(PairJob) * jobs.size(), sizeof(int4) * nitems,
+                                cudaMemcpyHostToDevice, st));
+        FS_CUDA(cudaStreamSynchronize(st));
+        sl.host = std::move(bytes);
+        sl.njobs = (int)jobs.size();
+        sl.nitems = nitems;
+    }
+
+    void launch(const Slot& sl, int R_) {
+        launch_pairs_batched(R_, pairs_batched_grid(R_), st, sl.jobs.p, sl.items.p, sl.nitems, counter.p, err.p);
+    }
+
+    static bool joins(const Sim& s) { return s.prm.field_kind == FS_FIELD_DIRECT32C; }
+
+    void run_call(int c, std::array<Slot, 4>& sl) {
+        std::vector<PairJob> jobs;
+        std::vector<Sim*> joined;
+        double w = 0;
+        for (auto& s : sims) {
+            s->pre_call(c);
+            const Sim::FieldCall fc = s->call(c);
+            PairJob j{};
+            if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, st, tpc, &j)) {
+                jobs.push_back(j);
+                joined.push_back(s.get());
+                w += s->field->last_pairs;
+            }
+            s->pairs += s->field->last_pairs;
+            s->evals += s->field->last_pairs;
+            pairs += s->field->last_pairs;
+        }
+        if (!jobs.empty()) {
+            stage(sl[c], jobs, R);
+            ProfScope prof("k_pairs32_batched", st, w);
+            launch(sl[c], R);
+        }
+        for (auto* s : joined) s->field->finalize(st);
+        for (auto& s : sims) s->post_call(c);
+    }
+
+    std::string mask() const {
+        std::string m(sims.size(), '0');
+        for (size_t i = 0; i < sims.size(); ++i)
+            if ((sims[i]->iter + 1) % sims[i]->prm.remesh_period == 0) m[i] = '1';
+        return m;
+    }
+
+    void step_direct(const std::string& key) {
+        auto& sl = slots[key];
+        for (int c = 0; c < 4; ++c) run_call(c, sl);
+    }
+
+    // Time the batched pair launch of the first field call for each
+    // candidate (targets per thread x source tiles per item); keep the fastest.
+    void autotune() {
+        tuned = true;
+        bool any = false;
+        for (auto& s : sims) any = any || joins(*s);
+        if (!any) return;
+        static const int kRs[] = {4, 8};
+        static const int kTpcs[] = {8, 16, 32, 64};
+        for (auto& s : sims)
+            if (joins(*s)) s->pre_call(0);  // stage-1 kernel; the step recomputes it
+        float best = 1e30f;
+        int bR = R, bT = tpc;
+        for (int r : kRs)
+            for (int t : kTpcs) {
+                std::vector<PairJob> jobs;
+                for (auto& s : sims) {
+                    if (!joins(*s)) continue;
+                    const Sim::FieldCall fc = s->call(0);
+                    PairJob j{};
+                    if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, st, t, &j)) jobs.push_back(j);
+                }
+                Slot sl;
+                stage(sl, jobs, r);
+                launch(sl, r);  // warm
+                FS_CUDA(cudaEventRecord(ev0, st));
+                launch(sl, r);
+                FS_CUDA(cudaEventRecord(ev1, st));
+                FS_CUDA(cudaEventSynchronize(ev1));
+                float ms = 0.f;
+                FS_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                if (ms < best) {
+                    best = ms;
+                    bR = r;
+                    bT = t;
+                }
+            }
+        R = bR;
+        tpc = bT;
+        slots.clear();
+        check();
+    }
+
+    void check() {
+        FS_CUDA(cudaStreamSynchronize(st));
+        int h = 0;
+        FS_CUDA(cudaMemcpy(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) {
+            FS_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+            fail((fs_status)h, "device wait timed out in the batched pair kernel");
+        }
+        for (auto& s : sims) s->check_status();
+    }
+
+    bool graphable() const {
+        for (auto& s : sims)
+            if (s->prm.field_kind != FS_FIELD_DIRECT32C && s->prm.field_kind != FS_FIELD_DIRECT64) return false;
+        return true;
+    }
+
+    // Capture one step of this mask.  Host bookkeeping done during the capture
+    // is kept (the graph is launched right after); on failure it is rolled back
+    // and false is returned.
+    bool capture(const std::string& key) {
+        struct Saved {
+            int iter;
+            double t, pairs, evals;
+            bool remeshing;
+        };
+        std::vector<Saved> saved;
+        for (auto& s : sims) saved.push_back({s->iter, s->t, s->pairs, s->evals, s->remeshing});
+        const double saved_pairs = pairs;
+        const long long l0 = fs_kernel_launches();
+        const unsigned long long e0 = alloc_epoch().load();
+        cudaGraph_t g = nullptr;
+        Graph G;
+        FS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        prof_capture_sink(&G.prof);
+        bool ok = true;
+        try {
+            step_direct(key);
+        } catch (...) {
+            ok = false;
+        }
+        prof_capture_sink(nullptr);
+        capturing = false;
+        const cudaError_t ee = cudaStreamEndCapture(st, &g);
+        if (ee != cudaSuccess) ok = false;
+        (void)cudaGetLastError();
+        if (ok && g && alloc_epoch().load() == e0) {
+            ok = cudaGraphInstantiate(&G.exec, g, 0) == cudaSuccess;
+            (void)cudaGetLastError();
+        } else {
+            ok = false;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (!ok) {
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+            prof_release(G.prof);
+            for (size_t i = 0; i < sims.size(); ++i) {
+                sims[i]->iter = saved[i].iter;
+                sims[i]->t = saved[i].t;
+                sims[i]->pairs = saved[i].pairs;
+                sims[i]->evals = saved[i].evals;
+                sims[i]->remeshing = saved[i].remeshing;
+            }
+            pairs = saved_pairs;
+            return false;
+        }
+        G.epoch = e0;
+        G.launches = fs_kernel_launches() - l0;
+        for (size_t i = 0; i < sims.size(); ++i) {
+            G.dpairs.push_back(sims[i]->pairs - saved[i].pairs);
+            G.devals.push_back(sims[i]->evals - saved[i].evals);
+        }
+        graphs[key] = std::move(G);
+        return true;
+    }
+
+    void replay_bookkeeping(const Graph& G) {
+        for (size_t i = 0; i < sims.size(); ++i) {
+            Sim& s = *sims[i];
+            s.iter += 1;
+            s.t += s.prm.dt;
+            s.remeshing = (s.iter % s.prm.remesh_period == 0);
+            s.pairs += G.dpairs[i];
+            s.evals += G.devals[i];
+            pairs += G.dpairs[i];
+        }
+    }
+
+    void step_one() {
+        if (sims.empty()) return;
+        if (!tuned) autotune();
+        const std::string key = mask();
+        FS_CUDA(cudaEventRecord(ev0, st));
+        bool done = false;
+        const Graph* launched = nullptr;
+        if (use_graphs && graphable() && warmed.count(key)) {
+            auto it = graphs.find(key);
+            if (it != graphs.end() && it->second.epoch != alloc_epoch().load()) {
+                cudaGraphExecDestroy(it->second.exec);
+                graphs.erase(it);
+                it = graphs.end();
+                warmed.erase(key);
+            }
+            if (it != graphs.end()) {
+                replay_bookkeeping(it->second);
+                FS_CUDA(cudaGraphLaunch(it->second.exec, st));
+                count_launches(it->second.launches);
+                launched = &it->second;
+                done = true;
+                ++graph_steps;
+            } else if (warmed.count(key) && !uncapturable.count(key)) {
+                if (capture(key)) {
+                    FS_CUDA(cudaGraphLaunch(graphs[key].exec, st));
+                    launched = &graphs[key];
+                    done = true;
+                    ++graph_steps;
+                } else {
+                    uncapturable.insert(key);
+                }
+            }
+        }
+        if (!done) {
+            step_direct(key);
+            warmed.insert(key);
+            ++plain_steps;
+        }
+        FS_CUDA(cudaEventRecord(ev1, st));
+        check();
+        if (launched) prof_harvest(launched->prof);
+        float ms = 0.f;
+        FS_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        step_ms.push_back(ms);
+    }
+};
+
+}  // namespace fsb
+
+struct fs_batch {
+    fsb::Batch impl;
+};
+
+extern "C" {
+
+fs_status fs_batch_create(int device, fs_batch** out) {
+    if (!out) return fsb::guard([] { fsb::fail(FS_ERR_ARG, "null argument"); });
+    *out = nullptr;
+    auto* b = new fs_batch();
+    fs_status rc = fsb::guard([&] { b->impl.init(device); });
+    if (rc != FS_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return FS_OK;
+}
+
+fs_status fs_batch_destroy(fs_batch* b) {
+    return fsb::guard([&] {
+        if (b) {
+            cudaSetDevice(b->impl.device);
+            delete b;
+        }
+    });
+}
+
+fs_status fs_batch_add(fs_batch* b, const fs_sim_params* params, int* id) {
+    return fsb::guard([&] {
+        if (!b || !params || !id) fsb::fail(FS_ERR_ARG, "null argument");
+        FS_CUDA(cudaSetDevice(b->impl.device));
+        *id = b->impl.add(*params);
+    });
+}
+
+fs_status fs_batch_remove(fs_batch* b, int id) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        FS_CUDA(cudaSetDevice(b->impl.device));
+        b->impl.remove(id);
+    });
+}
+
+fs_status fs_batch_step(fs_batch* b, int nsteps) {
+    return fsb::guard([&] {
+        if (!b || nsteps < 0) fsb::fail(FS_ERR_ARG, "bad argument");
+        FS_CUDA(cudaSetDevice(b->impl.device));
+        b->impl.step_ms.clear();
+        for (int k = 0; k < nsteps; ++k) b->impl.step_one();
+    });
+}
+
+fs_status fs_batch_export(fs_batch* b, int id, double* xs, double* ps, double* fs, double* q_ws, double* es) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        auto& S = *b->impl.sims[b->impl.index_of(id)];
+        FS_CUDA(cudaSetDevice(b->impl.device));
+        FS_CUDA(cudaStreamSynchronize(S.st));
+        const size_t n = sizeof(double) * S.N;
+        if (xs) FS_CUDA(cudaMemcpy(xs, S.x.p, n, cudaMemcpyDeviceToHost));
+        if (ps) FS_CUDA(cudaMemcpy(ps, S.p.p, n, cudaMemcpyDeviceToHost));
+        if (fs) FS_CUDA(cudaMemcpy(fs, S.f.p, n, cudaMemcpyDeviceToHost));
+        if (q_ws) FS_CUDA(cudaMemcpy(q_ws, S.qw.p, n, cudaMemcpyDeviceToHost));
+        if (es) FS_CUDA(cudaMemcpy(es, S.e.p, n, cudaMemcpyDeviceToHost));
+    });
+}
+
+fs_status fs_batch_info(fs_batch* b, int id, int* npoints, int* iter, double* t, double* pairs) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        auto& S = *b->impl.sims[b->impl.index_of(id)];
+        if (npoints) *npoints = S.N;
+        if (iter) *iter = S.iter;
+        if (t) *t = S.t;
+        if (pairs) *pairs = S.pairs;
+    });
+}
+
+fs_status fs_batch_step_times(fs_batch* b, double* ms, int cap, int* n) {
+    return fsb::guard([&] {
+        if (!b || !n) fsb::fail(FS_ERR_ARG, "null argument");
+        const auto& v = b->impl.step_ms;
+        const int k = std::min<int>((int)v.size(), std::max(cap, 0));
+        for (int i = 0; i < k && ms; ++i) ms[i] = v[i];
+        *n = k;
+    });
+}
+
+fs_status fs_batch_work(fs_batch* b, double* pairs) {
+    return fsb::guard([&] {
+        if (!b || !pairs) fsb::fail(FS_ERR_ARG, "null argument");
+        *pairs = b->impl.pairs;
+    });
+}
+
+fs_status fs_batch_stats(fs_batch* b, int* targets_per_thread, int* tiles_per_item, long long* graph_steps,
+                         long long* plain_steps) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        if (targets_per_thread) *targets_per_thread = b->impl.R;
+        if (tiles_per_item) *tiles_per_item = b->impl.tpc;
+        if (graph_steps) *graph_steps = b->impl.graph_steps;
+        if (plain_steps) *plain_steps = b->impl.plain_steps;
+    });
+}
+
+fs_status fs_batch_set_tuning(fs_batch* b, int targets_per_thread, int tiles_per_item) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        if (targets_per_thread != 4 && targets_per_thread != 8)
+            fsb::fail(FS_ERR_ARG, "targets_per_thread must be 4 or 8");
+        if (tiles_per_item < 1 || tiles_per_item > 4096) fsb::fail(FS_ERR_ARG, "tiles_per_item must be 1..4096");
+        FS_CUDA(cudaStreamSynchronize(b->impl.st));
+        b->impl.R = targets_per_thread;
+        b->impl.tpc = tiles_per_item;
+        b->impl.tuned = true;
+        b->impl.reset_graphs();
+    });
+}
+
+fs_status fs_batch_set_graphs(fs_batch* b, int on) {
+    return fsb::guard([&] {
+        if (!b) fsb::fail(FS_ERR_ARG, "null batch");
+        FS_CUDA(cudaStreamSynchronize(b->impl.st));
+        b->impl.use_graphs = (on != 0);
+        b->impl.reset_graphs();
     });
 }
 

@@ -78,7 +78,30 @@ void collect_locked() {
 
 bool profiling_enabled() { return g_prof.load(std::memory_order_relaxed); }
 
+namespace {
+thread_local std::vector<ProfNode>* t_sink = nullptr;
+}
+
+void prof_capture_sink(std::vector<ProfNode>* sink) { t_sink = sink; }
+
 ProfScope::ProfScope(const char* name, cudaStream_t st, double work) : name_(name), st_(st), work_(work) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st_, &cs) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    if (cs != cudaStreamCaptureStatusNone) {
+        if (!t_sink) return;
+        if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
+            if (a_) cudaEventDestroy(a_);
+            a_ = b_ = nullptr;
+            (void)cudaGetLastError();
+            return;
+        }
+        captured_ = true;
+        cudaEventRecordWithFlags(a_, st_, cudaEventRecordExternal);
+        return;
+    }
     if (!profiling_enabled()) return;
     if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess) {
         a_ = b_ = nullptr;
@@ -87,12 +110,40 @@ ProfScope::ProfScope(const char* name, cudaStream_t st, double work) : name_(nam
     }
     cudaEventRecord(a_, st_);
 }
-
 ProfScope::~ProfScope() {
     if (!a_) return;
+    if (captured_) {
+        cudaEventRecordWithFlags(b_, st_, cudaEventRecordExternal);
+        if (t_sink) t_sink->push_back({name_, a_, b_, work_});
+        return;
+    }
     cudaEventRecord(b_, st_);
     std::lock_guard<std::mutex> lk(g_prof_mu);
     g_pending.push_back({name_, a_, b_, work_});
+}
+
+void prof_harvest(const std::vector<ProfNode>& nodes) {
+    if (!profiling_enabled()) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (const auto& n : nodes) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, n.a, n.b) != cudaSuccess) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        Total& t = g_totals[n.name];
+        t.launches += 1;
+        t.ms += ms;
+        t.work += n.work;
+    }
+}
+
+void prof_release(std::vector<ProfNode>& nodes) {
+    for (auto& n : nodes) {
+        cudaEventDestroy(n.a);
+        cudaEventDestroy(n.b);
+    }
+    nodes.clear();
 }
 
 }  // namespace fsb

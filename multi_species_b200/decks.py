@@ -43,3 +43,54 @@ def bump_on_tail(h=9, ph=1, steps=50, amp=0.04):
                 species_list=[dict(sp, name="bulk", ics_type=9, pth=1.0, pstr=0.0, q=-0.9, m=0.9),
                               dict(sp, name="beam", ics_type=9, pth=0.5, pstr=4.5, q=-0.1, m=0.1),
                               dict(sp, name="ions", ics_type=9, pth=ION_PTH, pstr=0.0, amp=0.0, q=1.0, m=1836.0)])
+
+
+def _quantized_mesh(target_per_species, nsp, lo=2000, hi=200000):
+    """(h, ph) with h in 4..8, ph in 0..2 whose point count (2*2^h+1)*(2*2^(h+ph)+1)
+    is closest in log to the per-species target, with the instance total in
+    [lo, hi] (panel counts must be powers of two)."""
+    best = None
+    for h in range(4, 9):
+        for ph in range(0, 3):
+            n = (2 * 2 ** h + 1) * (2 * 2 ** (h + ph) + 1)
+            if not lo <= n * nsp <= hi:
+                continue
+            d = abs(math.log(n / target_per_species))
+            if best is None or d < best[0]:
+                best = (d, h, ph)
+    return best[1], best[2]
+
+
+def landau_batch(count=64, seed=0, steps=40):
+    """Independent Landau-damping instances of uneven size: amplitude
+    alpha ~ U[0.001, 0.1], k ~ U[0.3, 0.6] (L = 2 pi / k), 1-3 species
+    (electrons; ions of mass 1836; a 10% electron beam at v = 2), total points
+    log-uniform in [2k, 200k] quantised to power-of-two panel counts;
+    eps 0.05, dt 0.25, remesh every 5 steps, FP32-compensated direct sum."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    decks = []
+    for _ in range(count):
+        alpha = float(rng.uniform(0.001, 0.1))
+        k = float(rng.uniform(0.3, 0.6))
+        nsp = int(rng.integers(1, 4))
+        total = float(np.exp(rng.uniform(math.log(2000), math.log(200000))))
+        h, ph = _quantized_mesh(total / nsp, nsp)
+        L = 2 * math.pi / k
+        sp = dict(initial_height=h, p_height=ph, pmin=-6.0, pmax=6.0, normalized_wavenumber=1.0, pstr=0.0)
+        species = [dict(sp, name="electrons", ics_type=1, pth=1.0, amp=alpha, q=-1.0, m=1.0)]
+        if nsp >= 2:
+            species.append(dict(sp, name="ions", ics_type=1, pth=ION_PTH, amp=0.0, q=1.0, m=1836.0))
+        if nsp >= 3:
+            species.append(dict(sp, name="beam", ics_type=9, pth=0.5, pstr=2.0, amp=alpha, q=-0.1, m=0.1))
+        decks.append(dict(xmin=0.0, xmax=L, pmin=-6.0, pmax=6.0, bcs=0, greens_epsilon=0.05, dt=0.25,
+                          num_steps=steps, remesh_period=5, use_treecode=0, quadrature=0,
+                          field_backend="direct32c", species_list=species))
+    return decks
+
+
+def deck_points(deck):
+    """Total panel points of a uniform deck."""
+    return sum((2 * 2 ** s["initial_height"] + 1) * (2 * 2 ** (s["initial_height"] + s["p_height"]) + 1)
+               for s in deck["species_list"])

@@ -1,0 +1,159 @@
+"""Batched stepping of many simulations (fs_batch_*): results against each
+member stepped alone (fs_sim_step), graph replay against launch-by-launch
+stepping, membership changes, and members of other field kinds."""
+import numpy as np
+import pytest
+
+import multi_species_b200 as fs
+from multi_species_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _small_decks(count, seed):
+    out = []
+    for d in decks.landau_batch(count=count, seed=seed, steps=10):
+        for s in d["species_list"]:  # keep the members small: 1k-17k points each
+            s["initial_height"] = min(s["initial_height"], 5)
+            s["p_height"] = min(s["p_height"], 1)
+        out.append(d)
+    return out
+
+
+def _alone(deck, steps, backend="direct32c"):
+    sim = fs.Simulation(deck, backend)
+    sim.step(steps)
+    st = sim.state()
+    sim.close()
+    return st
+
+
+def test_batch_matches_members_alone():
+    ds = _small_decks(4, seed=3)
+    b = fs.Batch()
+    ids = [b.add(d) for d in ds]
+    b.step(7)  # remesh at step 5; steps 2-4 and 6-7 from graphs
+    st = b.stats()
+    assert st["graph_steps"] >= 4 and st["plain_steps"] >= 2, st
+    for i, d in zip(ids, ds):
+        got = b.state(i)
+        ref = _alone(d, 7)
+        assert b.info(i)["iter"] == 7
+        assert _rel(got["es"], ref["es"]) <= 1e-6
+        # the members' FP32 pair sums are split into chunks differently alone
+        # (tiles per item), so E differs at FP32 rounding level; positions
+        # integrate it, f and the weights interpolate at those positions
+        for k, tol in (("xs", 1e-8), ("ps", 1e-8), ("fs", 1e-7), ("q_ws", 1e-7)):
+            assert _rel(got[k], ref[k]) <= tol, k
+    b.close()
+
+
+def test_batch_fp32c_against_fp64():
+    ds = _small_decks(3, seed=5)
+    b = fs.Batch()
+    ids = [b.add(d) for d in ds]
+    b.step(1)
+    for i, d in zip(ids, ds):
+        ref = _alone(d, 1, "direct64")
+        assert _rel(b.state(i)["es"], ref["es"]) <= 1e-6
+    b.close()
+
+
+def test_graphs_replay_bit_identical():
+    ds = _small_decks(3, seed=7)
+    out = []
+    for graphs in (True, False):
+        b = fs.Batch(graphs=graphs, tuning=(4, 8))
+        ids = [b.add(d) for d in ds]
+        b.step(6)
+        out.append([b.state(i) for i in ids])
+        st = b.stats()
+        assert (st["graph_steps"] > 0) == graphs
+        b.close()
+    for a, c in zip(*out):
+        for k in a:
+            assert np.array_equal(a[k], c[k]), k
+
+
+def test_member_alone_and_in_mix_bit_identical():
+    ds = _small_decks(5, seed=11)
+    b1 = fs.Batch(tuning=(4, 16))
+    i1 = b1.add(ds[0])
+    b1.step(6)
+    alone = b1.state(i1)
+    b2 = fs.Batch(tuning=(4, 16))
+    ids = [b2.add(d) for d in ds]
+    b2.step(6)
+    mixed = b2.state(ids[0])
+    for k in alone:
+        assert np.array_equal(alone[k], mixed[k]), k
+    b1.close()
+    b2.close()
+
+
+def test_membership_changes_and_phases():
+    ds = _small_decks(4, seed=13)
+    b = fs.Batch(tuning=(8, 32))
+    a = b.add(ds[0])
+    c = b.add(ds[1])
+    b.step(3)
+    b.remove(c)
+    d = b.add(ds[2])  # joins at iteration 0 while `a` is at 3: remeshes fall on different steps
+    b.step(4)
+    assert b.info(a)["iter"] == 7 and b.info(d)["iter"] == 4
+    assert b.stats()["graph_steps"] > 0
+    with pytest.raises(fs.FsError):
+        b.info(c)
+    for sid, deck, steps in ((a, ds[0], 7), (d, ds[2], 4)):
+        ref = _alone(deck, steps)
+        got = b.state(sid)
+        assert _rel(got["es"], ref["es"]) <= 1e-6
+        assert _rel(got["xs"], ref["xs"]) <= 1e-8
+    b.close()
+
+
+def test_other_field_kinds_join_bit_identical():
+    ds = _small_decks(2, seed=17)
+    b = fs.Batch()
+    i64 = b.add(ds[0], "direct64")
+    i32 = b.add(ds[1])
+    b.step(6)
+    ref = _alone(ds[0], 6, "direct64")
+    got = b.state(i64)
+    for k in ref:
+        assert np.array_equal(got[k], ref[k]), k
+    assert _rel(b.state(i32)["es"], _alone(ds[1], 6)["es"]) <= 1e-6
+    b.close()
+
+
+def test_batch_argument_errors():
+    b = fs.Batch()
+    with pytest.raises(fs.FsError):
+        b.set_tuning(3, 8)
+    with pytest.raises(fs.FsError):
+        b.remove(12345)
+    b.step(0)
+    b.step(2)  # empty batch: nothing to do
+    b.close()
+
+
+def test_profile_counts_graph_replayed_launches():
+    ds = _small_decks(2, seed=19)
+    b = fs.Batch(tuning=(4, 16))
+    for d in ds:
+        b.add(d)
+    fs.profile_reset()
+    fs.profile_enable(True)
+    try:
+        b.step(4)  # step 1 launch by launch, step 2 captured, 3-4 replayed
+    finally:
+        fs.profile_enable(False)
+    n, ms, w = fs.profile_read("k_pairs32_batched")
+    assert b.stats()["graph_steps"] == 3
+    assert n == 16 and ms > 0
+    assert w == pytest.approx(b.pair_count(), rel=1e-12)
+    b.close()
