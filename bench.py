@@ -147,11 +147,17 @@ def measured_peaks():
 
 
 def traffic_per_pair(kernel: str):
-    """DRAM bytes per pair of the pair kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_traffic.json")
-    if os.path.exists(p):
+    """DRAM bytes per pair of a pair kernel, from the `dram_bytes_per_pair:` line
+    of its committed ncu summary (profiles/<kernel>_*.md)."""
+    import glob
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
         with open(p) as f:
-            return json.load(f)
+            lines = f.read().splitlines()
+        if f"kernel: {kernel}" not in lines:
+            continue
+        for line in lines:
+            if line.startswith("dram_bytes_per_pair:"):
+                return {"dram_bytes_per_pair": float(line.split(":")[1]), "source": os.path.basename(p)}
     return None
 
 
