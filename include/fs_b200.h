@@ -190,6 +190,71 @@ fs_status fs_batch_set_tuning(fs_batch* batch, int targets_per_thread, int tiles
 /* Graph capture on (default) or off; either way discards existing graphs. */
 fs_status fs_batch_set_graphs(fs_batch* batch, int on);
 
+/* ------------------------------------------------------------------ pool */
+/* Request loop for serving many simulations on one device (no counterpart in
+ * the reference).  Client threads submit (deck, steps) requests and return at
+ * once; one device-owner thread admits queued requests in arrival order while
+ * the estimated device bytes of the live members stay within
+ * hbm_budget_bytes and fewer than max_live are running, steps every live
+ * member together (an fs_batch underneath: their FP32 pair work shares one
+ * launch per field evaluation), and retires finished members (final state to
+ * host memory, device state freed).  Requests arriving while others run join
+ * at the next step.  All fs_pool_* calls are thread-safe. */
+typedef struct fs_pool_params {
+    int device;
+    double hbm_budget_bytes;      /* e.g. 150e9                                        */
+    int max_live;                 /* running requests at most (slots)                  */
+    int targets_per_thread;       /* 0: autotune on the first step; else 4 or 8        */
+    int tiles_per_item;           /* with targets_per_thread != 0: source tiles per item */
+} fs_pool_params;
+
+typedef enum fs_request_state {
+    FS_REQ_QUEUED = 0,
+    FS_REQ_RUNNING = 1,
+    FS_REQ_DONE = 2,
+    FS_REQ_FAILED = 3,
+    FS_REQ_CANCELLED = 4
+} fs_request_state;
+
+typedef struct fs_request_info {
+    int state;                    /* fs_request_state                                  */
+    int steps_done, nsteps, npoints;
+    double pairs;                 /* pair interactions evaluated for it                */
+    double step_ms_p50, step_ms_p99;  /* its per-step latencies (wall time of the steps it took part in) */
+    double queue_ms;              /* submit -> admission (-1 while queued)             */
+    double total_ms;              /* submit -> completion (-1 until finished)          */
+    char error[256];
+} fs_request_info;
+
+typedef struct fs_pool_stats_t {
+    long long submitted, admitted, completed, failed, cancelled, queued, live, iterations;
+    double hbm_in_use_bytes;      /* estimated bytes of the live members               */
+    double pairs;                 /* pair interactions of all requests                 */
+    double busy_ms;               /* wall time spent stepping                          */
+    double step_ms_p50, step_ms_p99;  /* over every (request, step)                    */
+} fs_pool_stats_t;
+
+typedef struct fs_pool fs_pool;
+
+fs_status fs_pool_create(const fs_pool_params* params, fs_pool** out);
+/* Stops the loop: queued and running requests are cancelled. */
+fs_status fs_pool_destroy(fs_pool* pool);
+/* Queue a simulation of params for nsteps steps.  FS_ERR_NOMEM when its
+ * estimate alone exceeds the budget. */
+fs_status fs_pool_submit(fs_pool* pool, const fs_sim_params* params, int nsteps, long long* id);
+fs_status fs_pool_cancel(fs_pool* pool, long long id);
+fs_status fs_pool_poll(fs_pool* pool, long long id, fs_request_info* info);
+/* Block until the request finished (timeout_ms < 0: no limit); *state gets its state. */
+fs_status fs_pool_wait(fs_pool* pool, long long id, double timeout_ms, int* state);
+/* Final state of a completed request (as fs_sim_export; any pointer may be NULL). */
+fs_status fs_pool_result(fs_pool* pool, long long id, double* xs, double* ps, double* fs, double* q_ws, double* es);
+/* Forget a finished request and its host copy of the state. */
+fs_status fs_pool_release(fs_pool* pool, long long id);
+fs_status fs_pool_step_times(fs_pool* pool, long long id, double* ms, int cap, int* n);
+fs_status fs_pool_stats(fs_pool* pool, fs_pool_stats_t* stats);
+/* Device bytes the pool reserves for a simulation of these parameters. */
+fs_status fs_pool_estimate_bytes(const fs_sim_params* params, double* bytes);
+
 /* ------------------------------------------------------------- host mesh */
 /* Sizes of the uniform periodic panel mesh of create_prerefined_mesh. */
 fs_status fs_mesh_sizes(int initial_height, int p_height, int* npoints, int* npanels, int* nleaves);

@@ -41,7 +41,9 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
            "fs_version", "fs_kernel_launches", "fs_batch_create", "fs_batch_destroy", "fs_batch_add",
            "fs_batch_remove", "fs_batch_step", "fs_batch_export", "fs_batch_info", "fs_batch_step_times",
-           "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs"]
+           "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
+           "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
+           "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes"]
 
 
 class FsError(RuntimeError):
@@ -67,6 +69,25 @@ class SimParams(C.Structure):
                 ("mac", C.c_double), ("degree", C.c_int), ("max_source", C.c_int), ("num_species", C.c_int),
                 ("species", SpeciesParams * 8), ("device", C.c_int)]
 
+
+class PoolParams(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_double), ("max_live", C.c_int),
+                ("targets_per_thread", C.c_int), ("tiles_per_item", C.c_int)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("steps_done", C.c_int), ("nsteps", C.c_int), ("npoints", C.c_int),
+                ("pairs", C.c_double), ("step_ms_p50", C.c_double), ("step_ms_p99", C.c_double),
+                ("queue_ms", C.c_double), ("total_ms", C.c_double), ("error", C.c_char * 256)]
+
+
+class PoolStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in ("submitted", "admitted", "completed", "failed", "cancelled", "queued",
+                                           "live", "iterations")] + \
+               [(n, C.c_double) for n in ("hbm_in_use_bytes", "pairs", "busy_ms", "step_ms_p50", "step_ms_p99")]
+
+
+REQUEST_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
 _lib = None
 _dp = C.POINTER(C.c_double)
@@ -118,6 +139,22 @@ def lib():
         L.fs_batch_stats.argtypes = [C.c_void_p, _ip, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.fs_batch_set_graphs.argtypes = [C.c_void_p, C.c_int]
         L.fs_batch_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        _llp = C.POINTER(C.c_longlong)
+        L.fs_pool_create.argtypes = [C.POINTER(PoolParams), C.POINTER(C.c_void_p)]
+        L.fs_pool_destroy.argtypes = [C.c_void_p]
+        L.fs_pool_submit.argtypes = [C.c_void_p, C.POINTER(SimParams), C.c_int, _llp]
+        L.fs_pool_cancel.argtypes = [C.c_void_p, C.c_longlong]
+        L.fs_pool_poll.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(RequestInfo)]
+        L.fs_pool_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, _ip]
+        L.fs_pool_result.argtypes = [C.c_void_p, C.c_longlong, _dp, _dp, _dp, _dp, _dp]
+        L.fs_pool_release.argtypes = [C.c_void_p, C.c_longlong]
+        L.fs_pool_step_times.argtypes = [C.c_void_p, C.c_longlong, _dp, C.c_int, _ip]
+        L.fs_pool_stats.argtypes = [C.c_void_p, C.POINTER(PoolStats)]
+        L.fs_pool_estimate_bytes.argtypes = [C.POINTER(SimParams), _dp]
+        for n in ("fs_pool_create", "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll",
+                  "fs_pool_wait", "fs_pool_result", "fs_pool_release", "fs_pool_step_times", "fs_pool_stats",
+                  "fs_pool_estimate_bytes"):
+            getattr(L, n).restype = st
         for n in ("fs_batch_create", "fs_batch_destroy", "fs_batch_add", "fs_batch_remove", "fs_batch_step",
                   "fs_batch_export", "fs_batch_info", "fs_batch_step_times", "fs_batch_work", "fs_batch_stats",
                   "fs_batch_set_tuning", "fs_batch_set_graphs"):
@@ -428,6 +465,87 @@ class Batch:
     def close(self) -> None:
         if getattr(self, "_h", None):
             lib().fs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------- serving
+def estimate_bytes(deck: dict, field_backend: str | None = None) -> float:
+    """Device bytes a Pool reserves for this deck (host-only computation)."""
+    p = sim_params(deck, field_backend)
+    v = C.c_double()
+    _check(lib().fs_pool_estimate_bytes(C.byref(p), C.byref(v)))
+    return v.value
+
+
+class Pool:
+    """Request loop serving many simulations on one GPU (fs_pool_*).
+
+    submit() queues a (deck, steps) request and returns its id at once; a
+    device-owner thread in the library admits requests in arrival order under
+    the HBM budget and slot count, steps all live requests together (their pair
+    work shares one launch per field evaluation) and retires finished ones.
+    Thread-safe.  No counterpart in the reference.
+    """
+
+    def __init__(self, device: int = 0, hbm_budget: float = 150e9, max_live: int = 64, tuning=None):
+        tpt, tpi = tuning if tuning is not None else (0, 0)
+        p = PoolParams(int(device), float(hbm_budget), int(max_live), int(tpt), int(tpi))
+        h = C.c_void_p()
+        _check(lib().fs_pool_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self.device = int(device)
+
+    def submit(self, deck: dict, steps: int, field_backend: str | None = None) -> int:
+        p = sim_params(deck, field_backend, self.device)
+        i = C.c_longlong()
+        _check(lib().fs_pool_submit(self._h, C.byref(p), int(steps), C.byref(i)))
+        return i.value
+
+    def cancel(self, rid: int) -> None:
+        _check(lib().fs_pool_cancel(self._h, int(rid)))
+
+    def poll(self, rid: int) -> dict:
+        r = RequestInfo()
+        _check(lib().fs_pool_poll(self._h, int(rid), C.byref(r)))
+        d = {f: getattr(r, f) for f, _ in RequestInfo._fields_ if f != "error"}
+        d["state"] = REQUEST_STATES[r.state]
+        d["error"] = r.error.decode(errors="replace")
+        return d
+
+    def wait(self, rid: int, timeout: float | None = None) -> str:
+        s = C.c_int()
+        _check(lib().fs_pool_wait(self._h, int(rid), -1.0 if timeout is None else 1e3 * timeout, C.byref(s)))
+        return REQUEST_STATES[s.value]
+
+    def result(self, rid: int) -> dict:
+        n = self.poll(rid)["npoints"]
+        a = {k: np.zeros(n) for k in ("xs", "ps", "fs", "q_ws", "es")}
+        _check(lib().fs_pool_result(self._h, int(rid), *(_ptr(a[k]) for k in ("xs", "ps", "fs", "q_ws", "es"))))
+        return a
+
+    def release(self, rid: int) -> None:
+        _check(lib().fs_pool_release(self._h, int(rid)))
+
+    def step_times(self, rid: int):
+        buf = np.zeros(100000)
+        n = C.c_int()
+        _check(lib().fs_pool_step_times(self._h, int(rid), _ptr(buf), len(buf), C.byref(n)))
+        return buf[: n.value].copy()
+
+    def stats(self) -> dict:
+        s = PoolStats()
+        _check(lib().fs_pool_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in PoolStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().fs_pool_destroy(self._h)
             self._h = None
 
     def __del__(self):

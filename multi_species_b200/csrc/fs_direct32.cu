@@ -217,6 +217,7 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // No square root is needed for far pairs, and the reciprocals of two pairs
 // come from one MUFU.RCP of their product: w_a = r_b / (r_a r_b).
 constexpr double kBand = 24.0;
+constexpr int kMaxChunks = 64;
 
 // One (target block, source chunk) of a job: kR targets per thread, the
 // chunk's tiles moved into shared memory by TMA bulk copies on two mbarriers.
@@ -507,7 +508,9 @@ class Direct32c final : public FieldEngine {
         const int ntiles = (ns + kS - 1) / kS;
         const int ns_pad = ntiles * kS;
         const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
-        tpc = std::max(1, tpc);
+        // at most kMaxChunks source chunks: bounds the partial sums to
+        // 8 * kMaxChunks bytes per target whatever the item shape
+        tpc = std::max(std::max(1, tpc), (ntiles + kMaxChunks - 1) / kMaxChunks);
         const int nchunks = ntiles ? (ntiles + tpc - 1) / tpc : 1;
         reserve(std::max(ns, 1), ns_pad, same ? 0 : nt, nt_pad, (size_t)nchunks * nt_pad, ntiles);
         const int T = 256;

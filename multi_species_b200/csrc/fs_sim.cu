@@ -31,7 +31,12 @@
 #include <algorithm>
 #include <cfloat>
 #include <climits>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <array>
 #include <map>
 #include <memory>
@@ -45,8 +50,11 @@ namespace fsb {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kWalkLimit = 4096;
-constexpr int kHist = 32;
+// A walk keeps every panel it visited in its own kHist-int slice of global
+// scratch (it stops at the first revisit, as the reference's visited set
+// does); a walk longer than kHist panels stops with FS_ERR_WALK instead of
+// forgetting where it has been.
+constexpr int kHist = 1024;
 
 __device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
 
@@ -168,17 +176,15 @@ __device__ __forceinline__ bool edge_bottom(double x_br, double p_br, double x_b
 // step to the neighbour across the first failed edge (right, top, bottom, left
 // priority), shifting tx by Lx across the periodic seam; stop at the first
 // panel already visited.  beyond_boundary is or-ed over every visited panel.
-// Bounded: returns -1 when the walk exceeds kWalkLimit steps.
+// Bounded: returns -1 when the walk visits more than kHist panels.
 __device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const double* __restrict__ op,
-                         double& tx, double tp, int leaf, bool& beyond) {
+                         double& tx, double tp, int leaf, bool& beyond, int* __restrict__ hist) {
     const double Lx = M.Lx;
     const int* R = M.rec;
-    int hist[kHist];
     int nh = 0;
     hist[nh++] = leaf;
-    for (int steps = 0;; ++steps) {
+    for (;;) {
         if (leaf == 0) return 0;
-        if (steps > kWalkLimit) return -1;
         const int* P = R + (size_t)leaf * 18;
         const double x_bl = ox[P[0]], p_bl = op[P[0]];
         const double x_tl = ox[P[2]], p_tl = op[P[2]];
@@ -211,10 +217,10 @@ __device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const
         if ((!ir && right == -2) || (!il && left == -2) || (!it && top == -2) || (!ib && bottom == -2))
             beyond = true;
         bool seen = false;
-        for (int h = 0; h < min(nh, kHist); ++h) seen |= (hist[h] == nl);
+        for (int h = 0; h < nh; ++h) seen |= (hist[h] == nl);
         if (seen) return nl;
-        hist[nh % kHist] = nl;
-        ++nh;
+        if (nh == kHist) return -1;
+        hist[nh++] = nl;
         leaf = nl;
     }
 }
@@ -391,7 +397,7 @@ __global__ void k_row_sort(int nx, int pow2, const int* __restrict__ row_pts, co
 __global__ void k_walk_first_column(MeshView M, int nx, int np, const double* __restrict__ ox,
                                     const double* __restrict__ op, double* __restrict__ sortx,
                                     const double* __restrict__ sortp, int* __restrict__ first_col,
-                                    int* __restrict__ leaf_of, int* __restrict__ status) {
+                                    int* __restrict__ leaf_of, int* __restrict__ hist, int* __restrict__ status) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     bool beyond = false;
     int leaf = find_from_root(M, ox, op, sortx[0], sortp[0], beyond);
@@ -403,7 +409,7 @@ __global__ void k_walk_first_column(MeshView M, int nx, int np, const double* __
         const int pt = ii * nx;
         beyond = false;
         double tx = sortx[pt];
-        leaf = walk_from(M, ox, op, tx, sortp[pt], leaf, beyond);
+        leaf = walk_from(M, ox, op, tx, sortp[pt], leaf, beyond, hist);
         if (leaf < 0) {
             raise_status(status, FS_ERR_WALK);
             return;
@@ -418,7 +424,8 @@ __global__ void k_walk_first_column(MeshView M, int nx, int np, const double* __
 // point's leaf (AMRStructure_interp.cpp:689-722).  One thread per row.
 __global__ void k_walk_rows(MeshView M, int nx, int np, const double* __restrict__ ox, const double* __restrict__ op,
                             double* __restrict__ sortx, const double* __restrict__ sortp,
-                            const int* __restrict__ first_col, int* __restrict__ leaf_of, int* __restrict__ status) {
+                            const int* __restrict__ first_col, int* __restrict__ leaf_of, int* __restrict__ hist,
+                            int* __restrict__ status) {
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= np) return;
     int lc = first_col[ii];
@@ -426,7 +433,7 @@ __global__ void k_walk_rows(MeshView M, int nx, int np, const double* __restrict
         const int pt = ii * nx + jj;
         bool beyond = false;
         double tx = sortx[pt];
-        lc = walk_from(M, ox, op, tx, sortp[pt], lc, beyond);
+        lc = walk_from(M, ox, op, tx, sortp[pt], lc, beyond, hist + (size_t)ii * kHist);
         if (lc < 0) {
             raise_status(status, FS_ERR_WALK);
             return;
@@ -505,7 +512,7 @@ struct SpeciesState {
     DevBuf<double> lat_x, lat_p, w0, coef, fnew;
     DevBuf<int> rec, leaf_slot, leaves, row_pts;
     DevBuf<double> sx, sortx, sortp;
-    DevBuf<int> order, leaf_of, first_col;
+    DevBuf<int> order, leaf_of, first_col, walk_hist;
     int nxl = 0, npl = 0, pow2 = 1;
     // reduced grid
     int nu = 0, roff = 0;
@@ -632,6 +639,7 @@ struct Sim {
             ss->order.ensure(ss->n);
             ss->leaf_of.ensure(ss->n);
             ss->first_col.ensure(ss->npl);
+            ss->walk_hist.ensure((size_t)ss->npl * kHist);
             ss->coef.ensure((size_t)ss->nleaves * 11);
             ss->fnew.ensure(ss->n);
             // reduced grid of the lattice: unique x (strictly increasing, as
@@ -790,9 +798,10 @@ struct Sim {
             k_row_sort<<<s->npl, 512, smem, st>>>(s->nxl, s->pow2, s->row_pts.p, s->sx.p, s->lat_p.p, s->sortx.p,
                                                   s->sortp.p, s->order.p);
             k_walk_first_column<<<1, 32, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
-                                                  s->first_col.p, s->leaf_of.p, status.p);
+                                                  s->first_col.p, s->leaf_of.p, s->walk_hist.p, status.p);
             k_walk_rows<<<blocks(s->npl, 64), 64, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
-                                                           s->sortp.p, s->first_col.p, s->leaf_of.p, status.p);
+                                                           s->sortp.p, s->first_col.p, s->leaf_of.p, s->walk_hist.p,
+                                                           status.p);
             k_eval_points<<<blocks(s->n), kT, 0, st>>>(M, s->sortx.p, s->sortp.p, s->order.p, s->leaf_of.p,
                                                        s->fnew.p);
             k_reset_points<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
@@ -1488,6 +1497,465 @@ fs_status fs_batch_set_graphs(fs_batch* b, int on) {
         FS_CUDA(cudaStreamSynchronize(b->impl.st));
         b->impl.use_graphs = (on != 0);
         b->impl.reset_graphs();
+    });
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Pool: a request loop over one Batch (continuous batching).
+//
+// Client threads submit simulations (deck parameters + number of steps) and
+// return at once.  One device-owner thread admits queued requests in arrival
+// order while the HBM budget (estimated bytes of live members) and the slot
+// count allow, steps every live member one step per iteration (their pair
+// work shares one persistent launch per field evaluation), and retires
+// members that reached their step count: the final state is copied to host
+// memory and the device state freed.  Requests that arrive while others are
+// running join at the next iteration.  Per-request step latencies are the
+// wall times of the iterations in which the request advanced.
+// ======================================================================
+namespace fsb {
+
+// Device bytes of a simulation of N points (state, stage buffers, mesh and
+// remesh arrays, FP32 field engine with at most 64 source chunks), with
+// margin; checked against cudaMemGetInfo in the tests.
+double estimate_sim_bytes(const fs_sim_params& P) {
+    double n = 0;
+    for (int s = 0; s < P.num_species && s < 8; ++s) {
+        const double h = P.species[s].initial_height, ph = P.species[s].p_height;
+        n += (2.0 * std::pow(2.0, h) + 1.0) * (2.0 * std::pow(2.0, h + ph) + 1.0);
+    }
+    double per_point = 1100.0;
+    if (P.field_kind == FS_FIELD_TREECODE64 || P.field_kind == FS_FIELD_TREECODE32C) per_point = 1400.0;
+    return n * per_point + 8.0 * 1024 * 1024;
+}
+
+struct Pool {
+    enum State { QUEUED = 0, RUNNING = 1, DONE = 2, FAILED = 3, CANCELLED = 4 };
+    struct Request {
+        long long id = 0;
+        fs_sim_params prm{};
+        int nsteps = 0;
+        State state = QUEUED;
+        int steps_done = 0;
+        int member = 0;  // batch id while running
+        double est_bytes = 0;
+        int npoints = 0;
+        double pairs = 0;
+        std::vector<double> step_ms;
+        std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
+        std::vector<double> xs, ps, fs, qws, es;  // final state
+        std::string error;
+        bool cancel = false;
+    };
+
+    int device = 0;
+    double budget = 0, in_use = 0;
+    int max_live = 64;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<long long> queue;
+    std::map<long long, std::unique_ptr<Request>> reqs;
+    std::vector<long long> live;
+    long long next_id = 1;
+    bool stopping = false;
+    std::string broken;
+    std::thread worker;
+    Batch batch;  // owned by the worker thread after start
+    std::vector<double> all_step_ms;
+    double pairs_done = 0, busy_ms = 0;
+    long long n_completed = 0, n_failed = 0, n_cancelled = 0, n_admitted = 0, iterations = 0;
+
+    void start(int dev, double hbm_budget, int slots, int tpt, int tpi) {
+        device = dev;
+        budget = hbm_budget;
+        max_live = slots;
+        batch.init(dev);
+        if (tpt) {
+            batch.R = tpt;
+            batch.tpc = tpi;
+            batch.tuned = true;
+        }
+        worker = std::thread([this] { run(); });
+    }
+
+    void stop() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stopping = true;
+        }
+        cv_work.notify_all();
+        if (worker.joinable()) worker.join();
+    }
+
+    long long submit(const fs_sim_params& P, int nsteps) {
+        auto r = std::make_unique<Request>();
+        r->prm = P;
+        r->prm.device = device;
+        r->nsteps = nsteps;
+        r->est_bytes = estimate_sim_bytes(P);
+        r->t_submit = std::chrono::steady_clock::now();
+        std::lock_guard<std::mutex> lk(mu);
+        if (!broken.empty()) fail(FS_ERR_STATE, "pool stopped after a device error: " + broken);
+        if (stopping) fail(FS_ERR_STATE, "pool is shutting down");
+        if (r->est_bytes > budget)
+            fail(FS_ERR_NOMEM, "request needs about " + std::to_string((long long)(r->est_bytes / 1e6)) +
+                                   " MB of device memory, above the pool's HBM budget");
+        r->id = next_id++;
+        const long long id = r->id;
+        queue.push_back(id);
+        reqs[id] = std::move(r);
+        cv_work.notify_all();
+        return id;
+    }
+
+    // --- worker side -------------------------------------------------------
+    void finish(Request& r, State st, const std::string& err = std::string()) {
+        r.state = st;
+        r.error = err;
+        r.t_done = std::chrono::steady_clock::now();
+        if (st == DONE) ++n_completed;
+        if (st == FAILED) ++n_failed;
+        if (st == CANCELLED) ++n_cancelled;
+    }
+
+    // Move the member's final state to host memory and free its device state.
+    void retire(Request& r, State st, const std::string& err = std::string()) {
+        if (st == DONE) {
+            auto& S = *batch.sims[batch.index_of(r.member)];
+            const size_t n = S.N;
+            r.xs.resize(n);
+            r.ps.resize(n);
+            r.fs.resize(n);
+            r.qws.resize(n);
+            r.es.resize(n);
+            FS_CUDA(cudaStreamSynchronize(batch.st));
+            FS_CUDA(cudaMemcpy(r.xs.data(), S.x.p, 8 * n, cudaMemcpyDeviceToHost));
+            FS_CUDA(cudaMemcpy(r.ps.data(), S.p.p, 8 * n, cudaMemcpyDeviceToHost));
+            FS_CUDA(cudaMemcpy(r.fs.data(), S.f.p, 8 * n, cudaMemcpyDeviceToHost));
+            FS_CUDA(cudaMemcpy(r.qws.data(), S.qw.p, 8 * n, cudaMemcpyDeviceToHost));
+            FS_CUDA(cudaMemcpy(r.es.data(), S.e.p, 8 * n, cudaMemcpyDeviceToHost));
+        }
+        batch.remove(r.member);
+        std::lock_guard<std::mutex> lk(mu);
+        in_use -= r.est_bytes;
+        live.erase(std::find(live.begin(), live.end(), r.id));
+        finish(r, st, err);
+    }
+
+    // Admit queued requests in arrival order while budget and slots allow.
+    void admit() {
+        for (;;) {
+            Request* r = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                while (!queue.empty() && reqs[queue.front()]->cancel) {
+                    finish(*reqs[queue.front()], CANCELLED);
+                    queue.pop_front();
+                }
+                if (queue.empty() || (int)live.size() >= max_live) return;
+                Request& f = *reqs[queue.front()];
+                if (in_use + f.est_bytes > budget) return;
+                size_t fr = 0, tot = 0;
+                if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (double)fr < f.est_bytes + 512.0 * 1024 * 1024) {
+                    if (!live.empty()) return;  // wait for a member to leave
+                }
+                (void)cudaGetLastError();
+                queue.pop_front();
+                r = &f;
+                in_use += f.est_bytes;
+                live.push_back(f.id);
+                f.state = RUNNING;
+                f.t_admit = std::chrono::steady_clock::now();
+                ++n_admitted;
+            }
+            try {
+                r->member = batch.add(r->prm);
+                r->npoints = batch.sims[batch.index_of(r->member)]->N;
+            } catch (const FsError& e) {
+                std::lock_guard<std::mutex> lk(mu);
+                in_use -= r->est_bytes;
+                live.erase(std::find(live.begin(), live.end(), r->id));
+                finish(*r, FAILED, e.msg);
+                cv_done.notify_all();
+            }
+            if (r->nsteps == 0 && r->state == RUNNING) retire(*r, DONE);
+        }
+    }
+
+    void iterate() {
+        admit();
+        std::vector<Request*> running;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (long long id : live) running.push_back(reqs[id].get());
+        }
+        for (Request* r : running)
+            if (r->cancel) retire(*r, CANCELLED);
+        running.erase(std::remove_if(running.begin(), running.end(), [](Request* r) { return r->state != RUNNING; }),
+                      running.end());
+        if (running.empty()) return;
+        const auto t0 = std::chrono::steady_clock::now();
+        std::vector<double> before;
+        for (Request* r : running) before.push_back(batch.sims[batch.index_of(r->member)]->pairs);
+        batch.step_one();
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            ++iterations;
+            busy_ms += ms;
+            for (size_t i = 0; i < running.size(); ++i) {
+                Request* r = running[i];
+                const double w = batch.sims[batch.index_of(r->member)]->pairs - before[i];
+                r->pairs += w;
+                pairs_done += w;
+                r->steps_done += 1;
+                r->step_ms.push_back(ms);
+                all_step_ms.push_back(ms);
+            }
+        }
+        for (Request* r : running)
+            if (r->steps_done >= r->nsteps) retire(*r, DONE);
+        cv_done.notify_all();
+    }
+
+    void fail_all_live(const std::string& why) {
+        std::vector<Request*> running;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (long long id : live) running.push_back(reqs[id].get());
+        }
+        for (Request* r : running) {
+            try {
+                retire(*r, FAILED, why);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(mu);
+                in_use -= r->est_bytes;
+                live.erase(std::find(live.begin(), live.end(), r->id));
+                finish(*r, FAILED, why);
+            }
+        }
+    }
+
+    void run() {
+        cudaSetDevice(device);
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stopping || !queue.empty() || !live.empty(); });
+                if (stopping) break;
+            }
+            try {
+                iterate();
+            } catch (const FsError& e) {
+                // a member's remesh failure or a timed-out wait: the members of
+                // this iteration cannot be told apart, so all of them fail
+                const std::string why = e.msg;
+                fail_all_live(why);
+                if (e.code == FS_ERR_CUDA) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    broken = why;
+                    for (long long id : queue) finish(*reqs[id], FAILED, "pool stopped: " + why);
+                    queue.clear();
+                }
+            } catch (const std::exception& e) {
+                fail_all_live(e.what());
+            }
+            cv_done.notify_all();
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!broken.empty()) break;
+            }
+        }
+        // shut down: cancel what is left
+        std::vector<Request*> running;
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (long long id : live) running.push_back(reqs[id].get());
+            for (long long id : queue) finish(*reqs[id], CANCELLED);
+            queue.clear();
+        }
+        for (Request* r : running) {
+            try {
+                retire(*r, CANCELLED);
+            } catch (...) {
+            }
+        }
+        cv_done.notify_all();
+    }
+
+    Request& get(long long id) {
+        auto it = reqs.find(id);
+        if (it == reqs.end()) fail(FS_ERR_ARG, "no request with id " + std::to_string(id));
+        return *it->second;
+    }
+
+    static double percentile(std::vector<double> v, double q) {
+        if (v.empty()) return 0.0;
+        std::sort(v.begin(), v.end());
+        const double pos = q * (v.size() - 1);
+        const size_t i = (size_t)pos;
+        const double f = pos - i;
+        return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+    }
+};
+
+}  // namespace fsb
+
+struct fs_pool {
+    fsb::Pool impl;
+};
+
+extern "C" {
+
+fs_status fs_pool_create(const fs_pool_params* params, fs_pool** out) {
+    if (!params || !out) return fsb::guard([] { fsb::fail(FS_ERR_ARG, "null argument"); });
+    *out = nullptr;
+    const fs_pool_params P = *params;
+    fs_status rc = fsb::guard([&] {
+        if (!(P.hbm_budget_bytes > 0)) fsb::fail(FS_ERR_ARG, "hbm_budget_bytes must be positive");
+        if (P.max_live < 1) fsb::fail(FS_ERR_ARG, "max_live must be >= 1");
+        if (P.targets_per_thread != 0 && P.targets_per_thread != 4 && P.targets_per_thread != 8)
+            fsb::fail(FS_ERR_ARG, "targets_per_thread must be 0 (autotune), 4 or 8");
+        if (P.targets_per_thread != 0 && P.tiles_per_item < 1) fsb::fail(FS_ERR_ARG, "tiles_per_item must be >= 1");
+    });
+    if (rc != FS_OK) return rc;
+    auto* p = new fs_pool();
+    rc = fsb::guard([&] {
+        FS_CUDA(cudaSetDevice(P.device));
+        p->impl.start(P.device, P.hbm_budget_bytes, P.max_live, P.targets_per_thread, P.tiles_per_item);
+    });
+    if (rc != FS_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return FS_OK;
+}
+
+fs_status fs_pool_destroy(fs_pool* p) {
+    return fsb::guard([&] {
+        if (!p) return;
+        p->impl.stop();
+        cudaSetDevice(p->impl.device);
+        delete p;
+    });
+}
+
+fs_status fs_pool_submit(fs_pool* p, const fs_sim_params* params, int nsteps, long long* id) {
+    return fsb::guard([&] {
+        if (!p || !params || !id) fsb::fail(FS_ERR_ARG, "null argument");
+        if (nsteps < 0) fsb::fail(FS_ERR_ARG, "nsteps must be >= 0");
+        if (params->num_species < 1 || params->num_species > 8) fsb::fail(FS_ERR_ARG, "num_species must be 1..8");
+        *id = p->impl.submit(*params, nsteps);
+    });
+}
+
+fs_status fs_pool_cancel(fs_pool* p, long long id) {
+    return fsb::guard([&] {
+        if (!p) fsb::fail(FS_ERR_ARG, "null pool");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        p->impl.get(id).cancel = true;
+        p->impl.cv_work.notify_all();
+    });
+}
+
+fs_status fs_pool_poll(fs_pool* p, long long id, fs_request_info* info) {
+    return fsb::guard([&] {
+        if (!p || !info) fsb::fail(FS_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        const auto& r = p->impl.get(id);
+        info->state = (int)r.state;
+        info->steps_done = r.steps_done;
+        info->nsteps = r.nsteps;
+        info->npoints = r.npoints;
+        info->pairs = r.pairs;
+        info->step_ms_p50 = fsb::Pool::percentile(r.step_ms, 0.5);
+        info->step_ms_p99 = fsb::Pool::percentile(r.step_ms, 0.99);
+        using ms = std::chrono::duration<double, std::milli>;
+        const bool admitted = r.state != fsb::Pool::QUEUED && r.t_admit.time_since_epoch().count() != 0;
+        info->queue_ms = admitted ? ms(r.t_admit - r.t_submit).count() : -1.0;
+        info->total_ms = (r.state >= fsb::Pool::DONE) ? ms(r.t_done - r.t_submit).count() : -1.0;
+        std::snprintf(info->error, sizeof(info->error), "%s", r.error.c_str());
+    });
+}
+
+fs_status fs_pool_wait(fs_pool* p, long long id, double timeout_ms, int* state) {
+    return fsb::guard([&] {
+        if (!p) fsb::fail(FS_ERR_ARG, "null pool");
+        std::unique_lock<std::mutex> lk(p->impl.mu);
+        auto done = [&] { return p->impl.get(id).state >= fsb::Pool::DONE; };
+        if (timeout_ms < 0) {
+            p->impl.cv_done.wait(lk, done);
+        } else {
+            p->impl.cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done);
+        }
+        if (state) *state = (int)p->impl.get(id).state;
+    });
+}
+
+fs_status fs_pool_result(fs_pool* p, long long id, double* xs, double* ps, double* fs, double* q_ws, double* es) {
+    return fsb::guard([&] {
+        if (!p) fsb::fail(FS_ERR_ARG, "null pool");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        auto& r = p->impl.get(id);
+        if (r.state != fsb::Pool::DONE) fsb::fail(FS_ERR_STATE, "request has not completed");
+        const size_t n = r.xs.size();
+        if (xs) std::memcpy(xs, r.xs.data(), 8 * n);
+        if (ps) std::memcpy(ps, r.ps.data(), 8 * n);
+        if (fs) std::memcpy(fs, r.fs.data(), 8 * n);
+        if (q_ws) std::memcpy(q_ws, r.qws.data(), 8 * n);
+        if (es) std::memcpy(es, r.es.data(), 8 * n);
+    });
+}
+
+fs_status fs_pool_release(fs_pool* p, long long id) {
+    return fsb::guard([&] {
+        if (!p) fsb::fail(FS_ERR_ARG, "null pool");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        auto& r = p->impl.get(id);
+        if (r.state < fsb::Pool::DONE) fsb::fail(FS_ERR_STATE, "request is still queued or running");
+        p->impl.reqs.erase(id);
+    });
+}
+
+fs_status fs_pool_step_times(fs_pool* p, long long id, double* ms, int cap, int* n) {
+    return fsb::guard([&] {
+        if (!p || !n) fsb::fail(FS_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        const auto& v = p->impl.get(id).step_ms;
+        const int k = std::min<int>((int)v.size(), std::max(cap, 0));
+        for (int i = 0; i < k && ms; ++i) ms[i] = v[i];
+        *n = k;
+    });
+}
+
+fs_status fs_pool_stats(fs_pool* p, fs_pool_stats_t* s) {
+    return fsb::guard([&] {
+        if (!p || !s) fsb::fail(FS_ERR_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(p->impl.mu);
+        auto& P = p->impl;
+        s->submitted = P.next_id - 1;
+        s->admitted = P.n_admitted;
+        s->completed = P.n_completed;
+        s->failed = P.n_failed;
+        s->cancelled = P.n_cancelled;
+        s->queued = (long long)P.queue.size();
+        s->live = (long long)P.live.size();
+        s->iterations = P.iterations;
+        s->hbm_in_use_bytes = P.in_use;
+        s->pairs = P.pairs_done;
+        s->busy_ms = P.busy_ms;
+        s->step_ms_p50 = fsb::Pool::percentile(P.all_step_ms, 0.5);
+        s->step_ms_p99 = fsb::Pool::percentile(P.all_step_ms, 0.99);
+    });
+}
+
+fs_status fs_pool_estimate_bytes(const fs_sim_params* params, double* bytes) {
+    return fsb::guard([&] {
+        if (!params || !bytes) fsb::fail(FS_ERR_ARG, "null argument");
+        *bytes = fsb::estimate_sim_bytes(*params);
     });
 }
 

@@ -1,0 +1,170 @@
+"""Serving pool (fs_pool_*): continuous batching of requests that arrive while
+others run, with admission by HBM budget and slots.  The key property: a
+request's result is the same alone and in the mix."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+import multi_species_b200 as fs
+from multi_species_b200 import decks
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _decks(count, seed, hmax=5):
+    out = []
+    for d in decks.landau_batch(count=count, seed=seed, steps=10):
+        for s in d["species_list"]:
+            s["initial_height"] = min(s["initial_height"], hmax)
+            s["p_height"] = min(s["p_height"], 1)
+        out.append(d)
+    return out
+
+
+def test_request_alone_and_in_mix_bit_identical():
+    ds = _decks(6, seed=23)
+    target = ds[0]
+    pool = fs.Pool(tuning=(4, 16))
+    rid = pool.submit(target, 12)
+    assert pool.wait(rid, timeout=120) == "done"
+    alone = pool.result(rid)
+    pool.close()
+
+    pool = fs.Pool(tuning=(4, 16))
+    early = [pool.submit(d, 15) for d in ds[1:3]]
+    time.sleep(0.2)  # the target arrives while these run
+    rid = pool.submit(target, 12)
+    late = [pool.submit(d, 8) for d in ds[3:]]
+    for r in early + [rid] + late:
+        assert pool.wait(r, timeout=300) == "done", pool.poll(r)
+    mixed = pool.result(rid)
+    info = pool.poll(rid)
+    assert info["steps_done"] == 12 and info["npoints"] == decks.deck_points(target)
+    for k in alone:
+        assert np.array_equal(alone[k], mixed[k]), k
+    st = pool.stats()
+    assert st["completed"] == 6 and st["failed"] == 0 and st["live"] == 0 and st["queued"] == 0
+    assert st["pairs"] == pytest.approx(sum(pool.poll(r)["pairs"] for r in early + [rid] + late), rel=1e-12)
+    assert 0 < st["step_ms_p50"] <= st["step_ms_p99"]
+    pool.close()
+
+    # and within the FP32 tolerance of the simulation stepped on its own
+    sim = fs.Simulation(target, "direct32c")
+    sim.step(12)
+    ref = sim.state()
+    sim.close()
+    assert _rel(mixed["es"], ref["es"]) <= 1e-6
+    assert _rel(mixed["xs"], ref["xs"]) <= 1e-8
+
+
+def test_autotuned_pool_matches_alone_within_tolerance():
+    ds = _decks(4, seed=29)
+    pool = fs.Pool()
+    ids = [pool.submit(d, 6) for d in ds]
+    for r in ids:
+        assert pool.wait(r, timeout=300) == "done", pool.poll(r)["error"]
+    for r, d in zip(ids, ds):
+        sim = fs.Simulation(d, "direct32c")
+        sim.step(6)
+        assert _rel(pool.result(r)["es"], sim.state()["es"]) <= 1e-6
+        sim.close()
+    pool.close()
+
+
+def test_budget_admission_serialises_requests():
+    ds = _decks(2, seed=31)
+    need = [fs.estimate_bytes(d) for d in ds]
+    pool = fs.Pool(hbm_budget=max(need) + 0.5 * min(need), tuning=(4, 16))  # one at a time
+    a = pool.submit(ds[0], 5)
+    b = pool.submit(ds[1], 5)
+    assert pool.wait(b, timeout=300) == "done", pool.poll(b)
+    assert pool.wait(a, timeout=300) == "done", pool.poll(a)
+    ia, ib = pool.poll(a), pool.poll(b)
+    assert ib["queue_ms"] >= ia["total_ms"] - 1.0  # b admitted only after a finished
+    assert pool.stats()["hbm_in_use_bytes"] == pytest.approx(0.0, abs=1.0)
+    with pytest.raises(fs.FsError):
+        pool.submit(decks.two_stream(h=8, ph=1), 1)  # alone above the budget
+    pool.close()
+
+
+def test_slots_limit_live_requests():
+    ds = _decks(5, seed=37, hmax=4)
+    pool = fs.Pool(max_live=2, tuning=(4, 16))
+    ids = [pool.submit(d, 4) for d in ds]
+    seen = 0
+    while not all(pool.poll(r)["state"] == "done" for r in ids):
+        seen = max(seen, pool.stats()["live"])
+        time.sleep(0.005)
+    assert seen <= 2
+    assert pool.stats()["completed"] == 5
+    pool.close()
+
+
+def test_cancel_and_release():
+    ds = _decks(2, seed=41)
+    pool = fs.Pool(tuning=(4, 16))
+    long_id = pool.submit(ds[0], 100000)
+    short = pool.submit(ds[1], 3)
+    assert pool.wait(short, timeout=120) == "done"
+    pool.cancel(long_id)
+    assert pool.wait(long_id, timeout=120) == "cancelled"
+    with pytest.raises(fs.FsError):
+        pool.result(long_id)
+    pool.release(short)
+    with pytest.raises(fs.FsError):
+        pool.poll(short)
+    assert pool.stats()["cancelled"] == 1
+    pool.close()
+
+
+def test_submit_from_many_threads():
+    ds = _decks(8, seed=43, hmax=4)
+    pool = fs.Pool(tuning=(8, 8))
+    ids, lock = [], threading.Lock()
+
+    def client(d):
+        r = pool.submit(d, 5)
+        with lock:
+            ids.append(r)
+        assert pool.wait(r, timeout=300) == "done"
+
+    th = [threading.Thread(target=client, args=(d,)) for d in ds]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert len(set(ids)) == 8
+    assert pool.stats()["completed"] == 8
+    pool.close()
+
+
+def test_destroy_with_work_in_flight():
+    ds = _decks(3, seed=47)
+    pool = fs.Pool(tuning=(4, 16))
+    for d in ds:
+        pool.submit(d, 100000)
+    time.sleep(0.3)
+    pool.close()  # cancels running and queued requests, frees their memory
+
+
+@pytest.mark.parametrize("backend,deck", [
+    ("direct32c", decks.landau_two_species(h=6, ph=1)),
+    ("direct32c", decks.two_stream(h=7, ph=1)),
+    ("treecode32c", decks.bump_on_tail(h=6, ph=1)),
+])
+def test_estimate_covers_device_memory(backend, deck):
+    import torch
+    torch.cuda.init()
+    free0, _ = torch.cuda.mem_get_info()
+    sim = fs.Simulation(deck, backend)
+    sim.step(5)  # includes a remesh
+    free1, _ = torch.cuda.mem_get_info()
+    sim.close()
+    used = free0 - free1
+    assert used <= fs.estimate_bytes(deck, backend), (used, fs.estimate_bytes(deck, backend))

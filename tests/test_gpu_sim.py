@@ -44,6 +44,22 @@ def test_remesh_step_matches_oracle():
     assert rel(a["es"], b["es"]) < 1e-11
 
 
+def test_remesh_with_long_walks_matches_oracle():
+    """A long-box Landau deck (L = 20.5, |v| up to 6, 5 steps of 0.25 before the
+    remesh) whose point location walks visit many panels before revisiting one;
+    every visited panel has to be remembered, as the reference's set does."""
+    d = decks.landau_batch(count=2, seed=29, steps=10)[1]
+    for s in d["species_list"]:
+        s["initial_height"], s["p_height"] = min(s["initial_height"], 5), min(s["p_height"], 1)
+    g, o = M.Simulation(d, "direct64"), O.Sim(d)
+    g.step(6)
+    o.step(6)
+    a, b = g.state(), o.state()
+    assert rel(a["fs"], b["fs"]) < 1e-12
+    assert rel(a["xs"], b["xs"]) < 1e-12
+    assert rel(a["es"], b["es"]) < 1e-11
+
+
 def test_remesh_only_matches_oracle_interpolation():
     """Remesh of a streamed two-stream state, species by species."""
     d = decks.two_stream(h=5, ph=1, remesh_period=1000)

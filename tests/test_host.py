@@ -56,3 +56,18 @@ def test_no_cpu_fallback_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(M, "_lib", None)
     with pytest.raises(ImportError):
         M.E_MQ_DirectSum_B200(1.0, 0.1)
+
+
+def test_pool_estimate_grows_with_points_and_rejects_bad_params():
+    from multi_species_b200 import decks
+    fs = M
+    small = fs.estimate_bytes(decks.landau_two_species(h=4, ph=0))
+    big = fs.estimate_bytes(decks.landau_two_species(h=7, ph=1))
+    assert 0 < small < big
+    # 2 species x 257 x 513 points at about 1.1 kB each
+    assert big == pytest.approx(2 * 257 * 513 * 1100 + 8 * 1024 * 1024)
+    tree = fs.estimate_bytes(decks.bump_on_tail(h=5, ph=1), "treecode32c")
+    assert tree > fs.estimate_bytes(decks.bump_on_tail(h=5, ph=1), "direct32c")
+    for kw in (dict(max_live=0), dict(hbm_budget=0.0), dict(tuning=(3, 8)), dict(tuning=(4, 0))):
+        with pytest.raises(fs.FsError):
+            fs.Pool(**kw)
