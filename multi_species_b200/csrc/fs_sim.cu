@@ -1096,6 +1096,19 @@ struct Batch {
         return next_id++;
     }
 
+    // Take a simulation created on its own stream (synchronised) into the
+    // batch: from now on it runs on the batch stream.
+    int adopt(std::unique_ptr<Sim> s) {
+        FS_CUDA(cudaStreamSynchronize(s->st));
+        if (s->own_stream) FS_CUDA(cudaStreamDestroy(s->st));
+        s->st = st;
+        s->own_stream = false;
+        sims.push_back(std::move(s));
+        ids.push_back(next_id);
+        reset_graphs();
+        return next_id++;
+    }
+
     int index_of(int id) const {
         for (size_t i = 0; i < ids.size(); ++i)
             if (ids[i] == id) return (int)i;
@@ -1554,15 +1567,17 @@ struct Pool {
     double budget = 0, in_use = 0;
     int max_live = 64;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
-    std::deque<long long> queue;
+    std::condition_variable cv_work, cv_prep, cv_done;
+    std::deque<long long> queue;                                       // submitted, not admitted
+    std::deque<std::pair<long long, std::unique_ptr<Sim>>> ready;      // created, not yet in the batch
     std::map<long long, std::unique_ptr<Request>> reqs;
-    std::vector<long long> live;
+    std::vector<long long> live;                                       // in the batch
+    int preparing = 0;
     long long next_id = 1;
     bool stopping = false;
     std::string broken;
-    std::thread worker;
-    Batch batch;  // owned by the worker thread after start
+    std::thread worker, preparer;
+    Batch batch;  // used by the worker thread only
     std::vector<double> all_step_ms;
     double pairs_done = 0, busy_ms = 0;
     long long n_completed = 0, n_failed = 0, n_cancelled = 0, n_admitted = 0, iterations = 0;
@@ -1578,6 +1593,7 @@ struct Pool {
             batch.tuned = true;
         }
         worker = std::thread([this] { run(); });
+        preparer = std::thread([this] { prepare_loop(); });
     }
 
     void stop() {
@@ -1586,6 +1602,8 @@ struct Pool {
             stopping = true;
         }
         cv_work.notify_all();
+        cv_prep.notify_all();
+        if (preparer.joinable()) preparer.join();
         if (worker.joinable()) worker.join();
     }
 
@@ -1606,11 +1624,26 @@ struct Pool {
         const long long id = r->id;
         queue.push_back(id);
         reqs[id] = std::move(r);
-        cv_work.notify_all();
+        cv_prep.notify_all();
         return id;
     }
 
-    // --- worker side -------------------------------------------------------
+    void cancel(long long id) {
+        std::lock_guard<std::mutex> lk(mu);
+        Request& r = get(id);
+        r.cancel = true;
+        if (r.state == QUEUED) {
+            auto it = std::find(queue.begin(), queue.end(), id);
+            if (it != queue.end()) {
+                queue.erase(it);
+                finish(r, CANCELLED);
+                cv_done.notify_all();
+            }
+        }
+        cv_work.notify_all();
+    }
+
+    // --- under mu -----------------------------------------------------------
     void finish(Request& r, State st, const std::string& err = std::string()) {
         r.state = st;
         r.error = err;
@@ -1619,7 +1652,68 @@ struct Pool {
         if (st == FAILED) ++n_failed;
         if (st == CANCELLED) ++n_cancelled;
     }
+    int occupied() const { return (int)live.size() + (int)ready.size() + preparing; }
+    bool front_fits() {
+        if (queue.empty() || occupied() >= max_live) return false;
+        return in_use + reqs[queue.front()]->est_bytes <= budget;
+    }
 
+    // --- preparer thread: admission and simulation set-up ---------------------
+    // Creating a simulation (host mesh, f0, upload, initial reduced field) runs
+    // on its own stream here, overlapping the worker's steps.
+    void prepare_loop() {
+        cudaSetDevice(device);
+        for (;;) {
+            Request* r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_prep.wait(lk, [&] { return stopping || !broken.empty() || front_fits(); });
+                if (stopping || !broken.empty()) return;
+                r = reqs[queue.front()].get();
+                size_t fr = 0, tot = 0;
+                if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (double)fr < r->est_bytes + 512.0 * 1024 * 1024 &&
+                    occupied() > 0) {
+                    // the device is fuller than the estimates say: wait for a member to leave
+                    cv_prep.wait_for(lk, std::chrono::milliseconds(50));
+                    continue;
+                }
+                (void)cudaGetLastError();
+                queue.pop_front();
+                in_use += r->est_bytes;
+                ++preparing;
+                r->state = RUNNING;
+                r->t_admit = std::chrono::steady_clock::now();
+                ++n_admitted;
+            }
+            std::unique_ptr<Sim> sim;
+            std::string err;
+            try {
+                sim = std::make_unique<Sim>();
+                sim->create(r->prm);
+            } catch (const FsError& e) {
+                err = e.msg.empty() ? "simulation set-up failed" : e.msg;
+            } catch (const std::exception& e) {
+                err = e.what();
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                --preparing;
+                if (!err.empty() || stopping) {
+                    in_use -= r->est_bytes;
+                    finish(*r, err.empty() ? CANCELLED : FAILED, err);
+                    sim.reset();
+                    cv_done.notify_all();
+                    cv_prep.notify_all();
+                } else {
+                    r->npoints = sim->N;
+                    ready.emplace_back(r->id, std::move(sim));
+                    cv_work.notify_all();
+                }
+            }
+        }
+    }
+
+    // --- worker thread ---------------------------------------------------------
     // Move the member's final state to host memory and free its device state.
     void retire(Request& r, State st, const std::string& err = std::string()) {
         if (st == DONE) {
@@ -1642,50 +1736,30 @@ struct Pool {
         in_use -= r.est_bytes;
         live.erase(std::find(live.begin(), live.end(), r.id));
         finish(r, st, err);
+        cv_prep.notify_all();
     }
 
-    // Admit queued requests in arrival order while budget and slots allow.
-    void admit() {
+    // Members created by the preparer join the batch.
+    void adopt_ready() {
         for (;;) {
+            std::pair<long long, std::unique_ptr<Sim>> item;
             Request* r = nullptr;
             {
+                // counted in `live` from here on, so the slot stays taken
                 std::lock_guard<std::mutex> lk(mu);
-                while (!queue.empty() && reqs[queue.front()]->cancel) {
-                    finish(*reqs[queue.front()], CANCELLED);
-                    queue.pop_front();
-                }
-                if (queue.empty() || (int)live.size() >= max_live) return;
-                Request& f = *reqs[queue.front()];
-                if (in_use + f.est_bytes > budget) return;
-                size_t fr = 0, tot = 0;
-                if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (double)fr < f.est_bytes + 512.0 * 1024 * 1024) {
-                    if (!live.empty()) return;  // wait for a member to leave
-                }
-                (void)cudaGetLastError();
-                queue.pop_front();
-                r = &f;
-                in_use += f.est_bytes;
-                live.push_back(f.id);
-                f.state = RUNNING;
-                f.t_admit = std::chrono::steady_clock::now();
-                ++n_admitted;
+                if (ready.empty()) return;
+                item = std::move(ready.front());
+                ready.pop_front();
+                r = reqs.at(item.first).get();
+                live.push_back(r->id);
             }
-            try {
-                r->member = batch.add(r->prm);
-                r->npoints = batch.sims[batch.index_of(r->member)]->N;
-            } catch (const FsError& e) {
-                std::lock_guard<std::mutex> lk(mu);
-                in_use -= r->est_bytes;
-                live.erase(std::find(live.begin(), live.end(), r->id));
-                finish(*r, FAILED, e.msg);
-                cv_done.notify_all();
-            }
-            if (r->nsteps == 0 && r->state == RUNNING) retire(*r, DONE);
+            r->member = batch.adopt(std::move(item.second));
+            if (r->nsteps == 0) retire(*r, DONE);
         }
     }
 
     void iterate() {
-        admit();
+        adopt_ready();
         std::vector<Request*> running;
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -1743,7 +1817,7 @@ struct Pool {
         for (;;) {
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] { return stopping || !queue.empty() || !live.empty(); });
+                cv_work.wait(lk, [&] { return stopping || !ready.empty() || !live.empty(); });
                 if (stopping) break;
             }
             try {
@@ -1751,13 +1825,13 @@ struct Pool {
             } catch (const FsError& e) {
                 // a member's remesh failure or a timed-out wait: the members of
                 // this iteration cannot be told apart, so all of them fail
-                const std::string why = e.msg;
-                fail_all_live(why);
+                fail_all_live(e.msg);
                 if (e.code == FS_ERR_CUDA) {
                     std::lock_guard<std::mutex> lk(mu);
-                    broken = why;
-                    for (long long id : queue) finish(*reqs[id], FAILED, "pool stopped: " + why);
+                    broken = e.msg;
+                    for (long long id : queue) finish(*reqs[id], FAILED, "pool stopped: " + e.msg);
                     queue.clear();
+                    cv_prep.notify_all();
                 }
             } catch (const std::exception& e) {
                 fail_all_live(e.what());
@@ -1768,7 +1842,7 @@ struct Pool {
                 if (!broken.empty()) break;
             }
         }
-        // shut down: cancel what is left
+        // shut down: what is left is cancelled
         std::vector<Request*> running;
         {
             std::lock_guard<std::mutex> lk(mu);
@@ -1782,6 +1856,17 @@ struct Pool {
             } catch (...) {
             }
         }
+        cv_done.notify_all();
+    }
+
+    void drain_ready_after_stop() {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& it : ready) {
+            Request& r = *reqs.at(it.first);
+            in_use -= r.est_bytes;
+            finish(r, CANCELLED);
+        }
+        ready.clear();
         cv_done.notify_all();
     }
 
@@ -1838,6 +1923,7 @@ fs_status fs_pool_destroy(fs_pool* p) {
     return fsb::guard([&] {
         if (!p) return;
         p->impl.stop();
+        p->impl.drain_ready_after_stop();
         cudaSetDevice(p->impl.device);
         delete p;
     });
@@ -1855,9 +1941,7 @@ fs_status fs_pool_submit(fs_pool* p, const fs_sim_params* params, int nsteps, lo
 fs_status fs_pool_cancel(fs_pool* p, long long id) {
     return fsb::guard([&] {
         if (!p) fsb::fail(FS_ERR_ARG, "null pool");
-        std::lock_guard<std::mutex> lk(p->impl.mu);
-        p->impl.get(id).cancel = true;
-        p->impl.cv_work.notify_all();
+        p->impl.cancel(id);
     });
 }
 

@@ -94,3 +94,50 @@ def deck_points(deck):
     """Total panel points of a uniform deck."""
     return sum((2 * 2 ** s["initial_height"] + 1) * (2 * 2 ** (s["initial_height"] + s["p_height"]) + 1)
                for s in deck["species_list"])
+
+
+def _quantized_heights(total, nsp, lo, hi):
+    """(h, ph) per species, h in 4..10, ph in 0..2, with nsp species of that
+    mesh totalling in [lo, hi] and closest in log to `total`."""
+    best = None
+    for h in range(4, 11):
+        for ph in range(0, 3):
+            n = nsp * (2 * 2 ** h + 1) * (2 * 2 ** (h + ph) + 1)
+            if not lo <= n <= hi:
+                continue
+            d = abs(math.log(n / total))
+            if best is None or d < best[0]:
+                best = (d, h, ph)
+    return best[1], best[2]
+
+
+def serving_requests(rate=20.0, seconds=60.0, seed=0, sigma=1.0):
+    """Poisson arrivals at `rate` per second for `seconds`; each request is a
+    Landau (two species, direct FP32c), two-stream (one species, direct FP32c)
+    or bump-on-tail (three species, FP32c treecode) deck with the parameters
+    of those workloads, total points log-normal with median 100k and log-sd
+    `sigma`, clipped to [10k, 2M] and quantised to power-of-two panel counts,
+    and 10-100 steps.  Returns [(arrival_s, kind, deck, steps)]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= seconds:
+            return out
+        kind = ("landau", "two_stream", "bump_on_tail")[int(rng.integers(0, 3))]
+        total = float(np.clip(np.exp(rng.normal(math.log(1e5), sigma)), 1e4, 2e6))
+        steps = int(rng.integers(10, 101))
+        nsp = {"landau": 2, "two_stream": 1, "bump_on_tail": 3}[kind]
+        h, ph = _quantized_heights(total, nsp, 10000, 2000000)
+        if kind == "landau":
+            d = landau_two_species(h=h, ph=ph, steps=steps)
+            d["field_backend"] = "direct32c"
+        elif kind == "two_stream":
+            d = two_stream(h=h, ph=ph, steps=steps)
+            d["field_backend"] = "direct32c"
+        else:
+            d = bump_on_tail(h=h, ph=ph, steps=steps)
+            d["field_backend"] = "treecode32c"
+        out.append((t, kind, d, steps))
