@@ -271,6 +271,18 @@ def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
     return roof
 
 
+def combine_ranks(total_ms, work):
+    """Replicas: the job's device time is the slowest rank's, its work the sum
+    over ranks (host scalars over the process group; no data-path collective)."""
+    import torch
+    import torch.distributed as D
+    t = torch.tensor([float(total_ms)], dtype=torch.float64)
+    D.all_reduce(t, op=D.ReduceOp.MAX)
+    w = torch.tensor([float(x) for x in work], dtype=torch.float64)
+    D.all_reduce(w, op=D.ReduceOp.SUM)
+    return float(t.item()), [float(x) for x in w.tolist()]
+
+
 def run_ours(a, rank, world, local_rank):
     import multi_species_b200 as M
     import torch
@@ -310,12 +322,7 @@ def run_ours(a, rank, world, local_rank):
     rl, rms, _ = M.profile_read("remesh")
     t_max = total_ms
     if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        t_max = float(t.item())
-        pw = torch.tensor([pairs, evals], dtype=torch.float64)
-        D.all_reduce(pw, op=D.ReduceOp.SUM)
-        pairs, evals = float(pw[0].item()), float(pw[1].item())
+        t_max, (pairs, evals) = combine_ranks(total_ms, [pairs, evals])
     value = pairs / (t_max / 1e3)
     res = None
     if rank == 0:
@@ -386,12 +393,7 @@ def run_batch(a, rank, world, local_rank):
     total_ms = float(np.sum(step_ms))
     t_max = total_ms
     if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64)
-        D.all_reduce(t, op=D.ReduceOp.MAX)
-        t_max = float(t.item())
-        pw = torch.tensor([pairs], dtype=torch.float64)
-        D.all_reduce(pw, op=D.ReduceOp.SUM)
-        pairs = float(pw[0].item())
+        t_max, (pairs,) = combine_ranks(total_ms, [pairs])
     value = pairs / (t_max / 1e3)
     if rank != 0:
         return None
