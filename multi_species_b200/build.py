@@ -38,6 +38,23 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def _defines() -> list:
+    """Extra -D flags from FS_B200_DEFINES ("NAME=VALUE NAME2=VALUE2"), for
+    building variants (e.g. FS_TILE_SOURCES=512); unset for the default build."""
+    return ["-D" + d for d in os.environ.get("FS_B200_DEFINES", "").split()]
+
+
+def _flags_changed() -> bool:
+    stamp = os.path.join(BUILD, "defines.txt")
+    now = " ".join(_defines())
+    old = open(stamp).read() if os.path.exists(stamp) else ""
+    if old != now:
+        with open(stamp, "w") as f:
+            f.write(now)
+        return True
+    return False
+
+
 def _headers_mtime() -> float:
     hs = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
         glob.glob(os.path.join(ROOT, "include", "*.h"))
@@ -49,11 +66,11 @@ def _compile(src: str, force: bool, verbose: bool, ptxas_v: bool) -> str:
     if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
             and os.path.getmtime(obj) >= _headers_mtime()):
         return obj
-    cmd = [nvcc()] + ARCH + COMMON + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + ARCH + COMMON + _defines() + ["-c", src, "-o", obj]
     if src.endswith(".cu") and ptxas_v:
         cmd += ["-Xptxas", "-v"]
     if src.endswith(".cpp"):
-        cmd = [nvcc(), "-x", "cu"] + ARCH + COMMON + ["-c", src, "-o", obj]
+        cmd = [nvcc(), "-x", "cu"] + ARCH + COMMON + _defines() + ["-c", src, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -67,6 +84,7 @@ def _compile(src: str, force: bool, verbose: bool, ptxas_v: bool) -> str:
 
 def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    force = _flags_changed() or force
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose, ptxas_v), srcs))

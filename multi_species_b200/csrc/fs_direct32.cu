@@ -46,7 +46,10 @@ namespace fsb {
 
 namespace {
 
-constexpr int kS = 256;          // sources per tile
+#ifndef FS_TILE_SOURCES
+#define FS_TILE_SOURCES 256
+#endif
+constexpr int kS = FS_TILE_SOURCES;  // sources per shared-memory tile
 constexpr int kNT = 128;         // threads per CTA
 constexpr int kRMax = 8;         // largest number of targets per thread
 constexpr int kTBPad = kNT * kRMax;  // target counts are padded to a multiple of this
@@ -211,12 +214,14 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
 // v = eps^2 w, w = 1/(d^2 + eps^2), v <= 1/(1 + kBand^2).  The sign part is
-// summed in FP64 (ffar); the pair kernel accumulates q/2 * c with
-// c = v/2 + v^2/8 = w (a1 + a2 w), a1 = eps^2/2, a2 = eps^4/8: the truncated
-// terms are below v^2/8 <= 4e-7 of c at the band edge and fall off as 1/d^4.
-// No square root is needed for far pairs, and the reciprocals of two pairs
-// come from one MUFU.RCP of their product: w_a = r_b / (r_a r_b).
-constexpr double kBand = 24.0;
+// summed in FP64 (ffar); the pair kernel accumulates q/2 * c with the shifted
+// form c = (v/2) / (1 - v/4) = a1 / (d^2 + 3 eps^2 / 4), a1 = eps^2/2, whose
+// series v/2 + v^2/8 + v^3/32 + ... matches c = v/2 + v^2/8 + v^3/16 + ... to
+// second order: the error is below v^2/16 <= 1e-6 of c at the band edge
+// (2e-9 of the pair's q/2) and falls off as 1/d^6.  Far pairs need no square
+// root and one FMA for the series, and two targets share one MUFU.RCP:
+// w'_a = r_b / (r_a r_b).
+constexpr double kBand = 16.0;
 constexpr int kMaxChunks = 64;
 
 // One (target block, source chunk) of a job: kR targets per thread, the
@@ -294,9 +299,9 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
         }
         const float4* tile = buf[b];
         if (!__any_sync(0xffffffffu, careful)) {
-            // far tiles: accumulate q/2 * c(v) = w (q/2 a1 + q/2 a2 w), two
-            // targets per packed FP32x2 op, one MUFU.RCP per two targets
-            const float2 e2v = make_float2(eps2, eps2);
+            // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
+            // two targets per packed FP32x2 op, one MUFU.RCP per two targets
+            const float2 e2v = make_float2(Jb.e2f, Jb.e2f);
             float2 tau2[kR / 2], acc2[kR / 2];
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
@@ -307,20 +312,22 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
                 const float2 nsx = make_float2(-e.x, -e.x);
-                const float2 qa1 = make_float2(e.z, e.z), qa2 = make_float2(e.w, e.w);
+                const float2 qa1 = make_float2(e.z, e.z);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
                     const float2 d = __fadd2_rn(tau2[h], nsx);
                     const float2 r2 = __ffma2_rn(d, d, e2v);
                     const float W = rcp_approx(r2.x * r2.y);
-                    const float2 w = __fmul2_rn(make_float2(r2.y, r2.x), make_float2(W, W));
-                    acc2[h] = __ffma2_rn(w, __ffma2_rn(w, qa2, qa1), acc2[h]);
+                    // (r_a W, r_b W) = (w'_b, w'_a): the lanes come out swapped,
+                    // so acc2[h].x accumulates target 2h+1 and .y target 2h
+                    const float2 w = __fmul2_rn(r2, make_float2(W, W));
+                    acc2[h] = __ffma2_rn(w, qa1, acc2[h]);
                 }
             }
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
-                acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].x;
-                acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].y;
+                acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
+                acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
             }
         } else {
             // near band / image split: per-pair image and band, Kahan sum of
@@ -400,6 +407,27 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
     }
 }
 
+// One job, persistent: a grid of one wave of CTAs takes (chunk, target block)
+// items in chunk-major order from an atomic counter, so the last, shorter
+// chunk comes last and no SM idles through a partial final wave.
+template <int kR>
+__global__ void __launch_bounds__(kNT) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
+                                                            int* __restrict__ counter, int* __restrict__ err) {
+    __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_item;
+    init_bars(bar);
+    uint32_t gk = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= nitems) break;
+        if (!pair_block<kR>(job, item % tblocks, item / tblocks, buf, bar, gk, err)) return;
+    }
+}
+
 // Targets per thread of the pair kernel: 2, 4 or 8 (register use vs. reuse of
 // each shared-memory source record).
 void launch_pairs(int R, dim3 grid, cudaStream_t st, const PairJob& job, int* err) {
@@ -407,6 +435,26 @@ void launch_pairs(int R, dim3 grid, cudaStream_t st, const PairJob& job, int* er
         case 2: k_pairs32<2><<<grid, kNT, 0, st>>>(job, err); break;
         case 8: k_pairs32<8><<<grid, kNT, 0, st>>>(job, err); break;
         default: k_pairs32<4><<<grid, kNT, 0, st>>>(job, err); break;
+    }
+}
+
+int persistent_grid(int R) {
+    int per_sm = 0;
+    switch (R) {
+        case 2: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_persistent<2>, kNT, 0)); break;
+        case 8: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_persistent<8>, kNT, 0)); break;
+        default: FS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pairs32_persistent<4>, kNT, 0)); break;
+    }
+    return std::max(1, per_sm) * sm_count();
+}
+
+void launch_pairs_persistent(int R, int grid, cudaStream_t st, const PairJob& job, int tblocks, int nitems,
+                             int* counter, int* err) {
+    FS_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+    switch (R) {
+        case 2: k_pairs32_persistent<2><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
+        case 8: k_pairs32_persistent<8><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
+        default: k_pairs32_persistent<4><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
     }
 }
 
@@ -482,18 +530,20 @@ class Direct32c final : public FieldEngine {
 
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
               cudaStream_t st) override {
-        // chunking for a standalone launch: enough CTAs for several waves
+        // a standalone launch: one persistent wave over about 32 items per CTA
         const int ntiles = (ns + kS - 1) / kS;
         const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
         const int tblocks = nt_pad / (kNT * R_);
-        const int want = sm_count() * 8 * 4;
+        if (!grid_) grid_ = persistent_grid(R_);
+        const int want = grid_ * 32;
         int nchunks = ntiles ? std::min(ntiles, std::max(1, (want + tblocks - 1) / tblocks)) : 1;
         const int tpc = ntiles ? (ntiles + nchunks - 1) / nchunks : 1;
         PairJob job;
         if (prepare(d_t, nt, d_s, d_q, ns, stage, st, tpc, &job)) {
             nchunks = (job.ntiles + job.tpc - 1) / job.tpc;
+            const int nitems = tblocks * nchunks;
             ProfScope prof("k_pairs32", st, last_pairs);
-            launch_pairs(R_, dim3(job.nt_pad / (kNT * R_), nchunks), st, job, err_.p);
+            launch_pairs_persistent(R_, std::min(grid_, nitems), st, job, tblocks, nitems, counter_.p, err_.p);
             FS_LAUNCHED(1);
         }
         finalize(st);
@@ -549,7 +599,7 @@ class Direct32c final : public FieldEngine {
                                                          info_.p);
         FS_LAUNCHED(1);
         *job = PairJob{src_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
-                       (float)(e2 / 2), (float)(e2 * e2 / 8), 0};
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2)};
         return true;
     }
 
@@ -581,6 +631,7 @@ class Direct32c final : public FieldEngine {
         if (!err_.p) {
             err_.ensure(1);
             FS_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
+            counter_.ensure(1);
         }
         const int nsort = std::max(ns, nt_sep);
         if (nt_sep) {
@@ -607,14 +658,15 @@ class Direct32c final : public FieldEngine {
         Stage stage;
     };
     double L_, eps_, cbg_;
-    int R_ = 4;
+    int R_ = 8;
+    int grid_ = 0;
     Fin fin_;
     DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
-    DevBuf<int> err_;
+    DevBuf<int> err_, counter_;
     DevBuf<unsigned char> cub_;
 };
 
@@ -767,7 +819,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
     const PairJob job{src, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
-                      (float)(e2 * e2 / 8), 0};
+                      (float)(e2 * e2 / 8), (float)(0.75 * e2)};
     launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;

@@ -167,8 +167,8 @@ struct PairJob {
     double* partial;          // chunks * nt_pad
     int ns, ntiles, tpc, nt_pad;
     double L;
-    float eps2, a1, a2;
-    int pad;
+    float eps2, a1, a2;  // near band: eps^2, eps^2/2, eps^4/8
+    float e2f;           // far pairs: 3 eps^2 / 4
 };
 
 class FieldEngine {
