@@ -389,6 +389,8 @@ def run_batch(a, rank, world, local_rank):
     launches = M.kernel_launches() - launches0
     pairs = b.pair_count() - pairs0
     kl, kms, kwork = M.profile_read("k_pairs32_batched")
+    breakdown = {k: M.profile_read(k)[1] / a.steps for k in ("k_pairs32_batched", "batch_prepare", "batch_finalize",
+                                                             "remesh")}
     stats = b.stats()
     b.close()
     total_ms = float(np.sum(step_ms))
@@ -426,6 +428,7 @@ def run_batch(a, rank, world, local_rank):
                               "points": decks.deck_points(big)},
            "speedup_vs_plain_fp64_gpu": value / plain,
            "step_ms_p50": float(np.percentile(step_ms, 50)), "step_ms_p99": float(np.percentile(step_ms, 99)),
+           "ms_per_step_by_phase": breakdown,
            "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
     if not a.no_e2e:
         res["e2e"] = e2e_plugin(big, "direct32c", decks.deck_points(big), local_rank)

@@ -1035,8 +1035,15 @@ struct Batch {
     };
     struct Capturing {};  // thrown when a captured step would need a host upload
 
+    // Members run their own work on kSide side streams (round robin), forked
+    // from and joined back into the batch stream around each phase, so small
+    // members' kernels overlap; the shared pair launch runs on `st`.
+    static constexpr int kSide = 8;
     int device = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kSide] = {};
+    int next_side = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<std::unique_ptr<Sim>> sims;
     std::vector<int> ids;
@@ -1057,9 +1064,16 @@ struct Batch {
     ~Batch() {
         reset_graphs();
         if (st) cudaStreamSynchronize(st);
+        for (auto& q : side)
+            if (q) cudaStreamSynchronize(q);
         sims.clear();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (auto& e : ev_join)
+            if (e) cudaEventDestroy(e);
+        for (auto& q : side)
+            if (q) cudaStreamDestroy(q);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -1069,6 +1083,11 @@ struct Batch {
         FS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         FS_CUDA(cudaEventCreate(&ev0));
         FS_CUDA(cudaEventCreate(&ev1));
+        FS_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        for (int k = 0; k < kSide; ++k) {
+            FS_CUDA(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+            FS_CUDA(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+        }
         counter.ensure(1);
         err.ensure(1);
         FS_CUDA(cudaMemset(err.p, 0, sizeof(int)));
@@ -1089,7 +1108,7 @@ struct Batch {
         if (P.device != device) fail(FS_ERR_ARG, "simulation device differs from the batch device");
         FS_CUDA(cudaStreamSynchronize(st));
         auto s = std::make_unique<Sim>();
-        s->create(P, st);
+        s->create(P, side[next_side++ % kSide]);
         sims.push_back(std::move(s));
         ids.push_back(next_id);
         reset_graphs();
@@ -1097,11 +1116,11 @@ struct Batch {
     }
 
     // Take a simulation created on its own stream (synchronised) into the
-    // batch: from now on it runs on the batch stream.
+    // batch: from now on it runs on one of the batch's side streams.
     int adopt(std::unique_ptr<Sim> s) {
         FS_CUDA(cudaStreamSynchronize(s->st));
         if (s->own_stream) FS_CUDA(cudaStreamDestroy(s->st));
-        s->st = st;
+        s->st = side[next_side++ % kSide];
         s->own_stream = false;
         sims.push_back(std::move(s));
         ids.push_back(next_id);
@@ -1164,30 +1183,52 @@ struct Batch {
 
     static bool joins(const Sim& s) { return s.prm.field_kind == FS_FIELD_DIRECT32C; }
 
+    void fork() {
+        FS_CUDA(cudaEventRecord(ev_fork, st));
+        for (int k = 0; k < kSide; ++k) FS_CUDA(cudaStreamWaitEvent(side[k], ev_fork, 0));
+    }
+    void join() {
+        for (int k = 0; k < kSide; ++k) {
+            FS_CUDA(cudaEventRecord(ev_join[k], side[k]));
+            FS_CUDA(cudaStreamWaitEvent(st, ev_join[k], 0));
+        }
+    }
+
     void run_call(int c, std::array<Slot, 4>& sl) {
         std::vector<PairJob> jobs;
         std::vector<Sim*> joined;
         double w = 0;
-        for (auto& s : sims) {
-            s->pre_call(c);
-            const Sim::FieldCall fc = s->call(c);
-            PairJob j{};
-            if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, st, tpc, &j)) {
-                jobs.push_back(j);
-                joined.push_back(s.get());
-                w += s->field->last_pairs;
+        {
+            // members' work before the shared launch, each on its side stream:
+            // RK stage, remesh, sort, source records, band searches (and whole
+            // evaluations of members that do not join)
+            ProfScope prof("batch_prepare", st);
+            fork();
+            for (auto& s : sims) {
+                s->pre_call(c);
+                const Sim::FieldCall fc = s->call(c);
+                PairJob j{};
+                if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, s->st, tpc, &j)) {
+                    jobs.push_back(j);
+                    joined.push_back(s.get());
+                    w += s->field->last_pairs;
+                }
+                s->pairs += s->field->last_pairs;
+                s->evals += s->field->last_pairs;
+                pairs += s->field->last_pairs;
             }
-            s->pairs += s->field->last_pairs;
-            s->evals += s->field->last_pairs;
-            pairs += s->field->last_pairs;
+            join();
         }
         if (!jobs.empty()) {
             stage(sl[c], jobs, R);
             ProfScope prof("k_pairs32_batched", st, w);
             launch(sl[c], R);
         }
-        for (auto* s : joined) s->field->finalize(st);
+        ProfScope prof("batch_finalize", st);
+        fork();
+        for (auto* s : joined) s->field->finalize(s->st);
         for (auto& s : sims) s->post_call(c);
+        join();
     }
 
     std::string mask() const {
@@ -1211,19 +1252,23 @@ struct Batch {
         if (!any) return;
         static const int kRs[] = {4, 8};
         static const int kTpcs[] = {8, 16, 32, 64};
+        fork();
         for (auto& s : sims)
             if (joins(*s)) s->pre_call(0);  // stage-1 kernel; the step recomputes it
+        join();
         float best = 1e30f;
         int bR = R, bT = tpc;
         for (int r : kRs)
             for (int t : kTpcs) {
+                fork();
                 std::vector<PairJob> jobs;
                 for (auto& s : sims) {
                     if (!joins(*s)) continue;
                     const Sim::FieldCall fc = s->call(0);
                     PairJob j{};
-                    if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, st, t, &j)) jobs.push_back(j);
+                    if (s->field->prepare(fc.x, fc.n, fc.x, fc.q, fc.n, fc.stage, s->st, t, &j)) jobs.push_back(j);
                 }
+                join();
                 Slot sl;
                 stage(sl, jobs, r);
                 launch(sl, r);  // warm
