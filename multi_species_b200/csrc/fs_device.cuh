@@ -67,4 +67,17 @@ __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
 // Bounded spin limit for every device-side wait (mbarrier, flags).
 constexpr long long kSpinLimit = 1LL << 26;
 
+// One MUFU.RSQ (callers pass arguments >= eps^2 > 0, never denormal).
+__device__ __forceinline__ float rsqrt_approx(float v) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+}
+// One MUFU.RCP (callers pass products of two values in [eps^2, L^2/4+eps^2]).
+__device__ __forceinline__ float rcp_approx(float v) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+}
+
 }  // namespace fsb

@@ -95,18 +95,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
-// One MUFU.RSQ: the argument is >= eps^2 > 0, never denormal.
-__device__ __forceinline__ float rsqrt_approx(float v) {
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
-    return y;
-}
-// One MUFU.RCP: the argument is a product of two values in [eps^2, L^2/4+eps^2].
-__device__ __forceinline__ float rcp_approx(float v) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v));
-    return y;
-}
 
 __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_double((long long)k); }
 

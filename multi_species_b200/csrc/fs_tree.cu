@@ -448,19 +448,25 @@ __global__ void k_far32(const TNode* __restrict__ nodes, const int* __restrict__
     efar[j] = norm * far;
 }
 
-// FP32-compensated form, near part: one CTA per (leaf, 256-target block).
-// Per target and near leaf the leaf's sorted sources are cut where their
-// periodic image changes (at most three images: a leaf spans < 2L + 0.2), and
-// within each image the same exact split as the direct FP32 kernel is used:
+// FP32-compensated form, near part: one CTA per (leaf, block of
+// kNearThreads x kNearR targets), kNearR targets per thread.
 //   K_tc(d) / norm = d/(2 sqrt(d^2+eps^2)) - c d,  d = xt - x_j  (xt = image of x_i)
-//   * the linear term c d and, for |d| > band, the sign part sign(d) lambda/2
-//     are summed exactly in FP64 from prefix sums of lambda and lambda x;
-//   * the kernel accumulates, in FP32 with Kahan compensation, lambda/2 d y for
-//     |d| <= band and -+ lambda/2 c(v) (c = v/2 + v^2/8, v = eps^2 y^2) beyond.
+// The linear term c d is summed exactly in FP64 from prefix sums of lambda and
+// lambda x.  For each near leaf, when every target of the CTA sees the whole
+// leaf in one periodic image and within the band |d| <= band (the usual case:
+// near leaves are neighbours a few leaf widths away), the pairs are
+// lambda/2 d y, y = rsqrt(d^2+eps^2), accumulated in packed FP32x2 over two
+// targets with Kahan compensation per tile and reduced in FP64 across tiles.
+// Otherwise every target of the CTA takes the general path for that leaf: the
+// leaf's sources are cut where their image changes (at most three images), and
+// beyond the band the sign part sign(d) lambda/2 is summed exactly in FP64 while
+// the kernel accumulates -+ lambda/2 c(v) (c = v/2 + v^2/8, v = eps^2 y^2).
 // Sources are staged through shared memory as FP32 offsets from an FP64 tile
 // base; each image's target offset is formed in FP64 before rounding.
-constexpr int kNearThreads = 256;
-constexpr int kNearTile = 512;
+constexpr int kNearThreads = 128;
+constexpr int kNearR = 4;
+constexpr int kNearBlock = kNearThreads * kNearR;
+constexpr int kNearTile = 256;
 constexpr double kNearBand = 24.0;
 
 struct NearImage {
@@ -477,10 +483,95 @@ __device__ __forceinline__ int lower_bound_d(const double* __restrict__ a, int l
     }
     return lo;
 }
+__device__ __forceinline__ int upper_bound_d(const double* __restrict__ a, int lo, int hi, double v) {
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (a[mid] <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
 __device__ __forceinline__ double range_sum(const double* __restrict__ incl, int a, int e) {
     // sum over [a, e) of the series whose inclusive prefix is incl
     if (e <= a) return 0.0;
     return incl[e - 1] - (a > 0 ? incl[a - 1] : 0.0);
+}
+
+// General path for one target and one near leaf (all threads of the CTA call
+// it together: it stages tiles through `sh` with barriers).
+__device__ void near_general(const TNode& nd, double x, const double* __restrict__ sx,
+                             const double* __restrict__ lam, const double* __restrict__ pl,
+                             const double* __restrict__ plx, double L, double band, double cbg, float eps2, float a1,
+                             float a2, float4* sh, double& exact, double& fp, int* __restrict__ err) {
+    NearImage im[3];
+    int nim = 0;
+    int a = nd.m0;
+    while (a <= nd.m1 && nim < 3) {
+        // image of source j: m_j = round((x - x_j) / L), the reference's
+        // choice (z - round(z)); m_j is non-increasing in j
+        const double m = round((x - sx[a]) / L);
+        const double xt = x - m * L;
+        int e;  // first source of the next image
+        {
+            int lo = a + 1, hi = nd.m1 + 1;
+            while (lo < hi) {
+                const int mid = lo + ((hi - lo) >> 1);
+                if (round((x - sx[mid]) / L) < m) hi = mid;
+                else lo = mid + 1;
+            }
+            e = lo;
+        }
+        const int U1 = lower_bound_d(sx, a, e, xt - band);
+        const int U2 = upper_bound_d(sx, U1, e, xt + band);  // first x_j > xt + band
+        exact += 0.5 * (range_sum(pl, a, U1) - range_sum(pl, U2, e)) -
+                 cbg * (xt * range_sum(pl, a, e) - range_sum(plx, a, e));
+        im[nim].xt = xt;
+        im[nim].start = a;
+        im[nim].U1 = U1;
+        im[nim].U2 = U2;
+        ++nim;
+        a = e;
+    }
+    if (a <= nd.m1) atomicCAS(err, 0, (int)FS_ERR_TREE);
+    for (int k = nim; k < 3; ++k) {
+        im[k].xt = im[nim - 1].xt;
+        im[k].start = INT_MAX;
+        im[k].U1 = im[k].U2 = 0;
+    }
+    for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile) {
+        const int cnt = min(kNearTile, nd.m1 - t0 + 1);
+        const double base = sx[t0];
+        __syncthreads();
+        for (int k = threadIdx.x; k < cnt; k += kNearThreads) {
+            const float lh = (float)(0.5 * lam[t0 + k]);
+            sh[k] = make_float4((float)(sx[t0 + k] - base), lh, lh * a1, lh * a2);
+        }
+        __syncthreads();
+        const float tau0 = (float)(im[0].xt - base), tau1 = (float)(im[1].xt - base),
+                    tau2 = (float)(im[2].xt - base);
+        const int s1 = im[1].start, s2 = im[2].start;
+        const int u10 = im[0].U1, u11 = im[1].U1, u12 = im[2].U1;
+        const int u20 = im[0].U2, u21 = im[1].U2, u22 = im[2].U2;
+        float acc = 0.f, cmp = 0.f;
+        for (int k = 0; k < cnt; ++k) {
+            const int jj = t0 + k;
+            const bool g1 = jj >= s1, g2 = jj >= s2;
+            const float tr = g2 ? tau2 : (g1 ? tau1 : tau0);
+            const int U1 = g2 ? u12 : (g1 ? u11 : u10);
+            const int U2 = g2 ? u22 : (g1 ? u21 : u20);
+            const float4 e = sh[k];
+            const float d = tr - e.x;
+            const float y = rsqrt_approx(fmaf(d, d, eps2));
+            const float z = y * y;
+            const float c = z * fmaf(z, e.w, e.z);
+            const float v = (jj < U1) ? -c : ((jj >= U2) ? c : e.y * (d * y));
+            const float w = v - cmp;
+            const float t = acc + w;
+            cmp = (t - acc) - w;
+            acc = t;
+        }
+        fp += (double)acc - (double)cmp;
+    }
 }
 
 __global__ void __launch_bounds__(kNearThreads)
@@ -489,93 +580,88 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
          const double* __restrict__ lam, const double* __restrict__ pl, const double* __restrict__ plx,
          const double* __restrict__ efar, const int* __restrict__ sidx, double L, double eps, double cbg, double norm,
          Stage S, int* __restrict__ err) {
-    __shared__ float4 sh[kNearTile];  // {s, lambda/2, lambda/2 a1, lambda/2 a2}
+    __shared__ float4 shg[kNearTile];          // general path: {s, lambda/2, lambda/2 a1, lambda/2 a2}
+    __shared__ float2 shb[kNearTile];          // band path: {s, lambda/2}
     const int l = blockIdx.x;
     if (l >= meta[1] || meta[2]) return;
     const TNode leaf = nodes[leaves[l]];
-    if (leaf.m0 + (int)blockIdx.y * kNearThreads > leaf.m1) return;  // whole CTA beyond the leaf
-    const int j = leaf.m0 + blockIdx.y * kNearThreads + threadIdx.x;
-    const bool active = j <= leaf.m1;
-    const double x = active ? sx[j] : sx[leaf.m0];
+    const int tb0 = leaf.m0 + (int)blockIdx.y * kNearBlock;
+    if (tb0 > leaf.m1) return;  // whole CTA beyond the leaf
     const double band = kNearBand * eps;
     const double e2d = eps * eps;
     const float eps2 = (float)e2d, a1 = (float)(e2d / 2), a2 = (float)(e2d * e2d / 8);
-    double exact = 0.0, fp = 0.0;
+    int jt[kNearR];
+    double x[kNearR], exact[kNearR], fp[kNearR];
+#pragma unroll
+    for (int r = 0; r < kNearR; ++r) {
+        jt[r] = tb0 + threadIdx.x + r * kNearThreads;
+        x[r] = (jt[r] <= leaf.m1) ? sx[jt[r]] : sx[leaf.m0];  // padded targets repeat a real one
+        exact[r] = 0.0;
+        fp[r] = 0.0;
+    }
     for (int q = 0; q < near_n[l]; ++q) {
         const TNode nd = nodes[near_list[(size_t)l * kNearCap + q]];
-        // images of this leaf's sources for this target
-        NearImage im[3];
-        int nim = 0;
-        int a = nd.m0;
-        while (a <= nd.m1 && nim < 3) {
-            // image of source j: m_j = round((x - x_j) / L), the reference's
-            // choice (z - round(z)); m_j is non-increasing in j
-            const double m = round((x - sx[a]) / L);
-            const double xt = x - m * L;
-            int e;  // first source of the next image
-            {
-                int lo = a + 1, hi = nd.m1 + 1;
-                while (lo < hi) {
-                    const int mid = lo + ((hi - lo) >> 1);
-                    if (round((x - sx[mid]) / L) < m) hi = mid;
-                    else lo = mid + 1;
+        const double xlo = sx[nd.m0], xhi = sx[nd.m1];
+        double xt[kNearR];
+        bool simple = true;
+#pragma unroll
+        for (int r = 0; r < kNearR; ++r) {
+            const double m = round((x[r] - xlo) / L);
+            xt[r] = x[r] - m * L;
+            simple = simple && (round((x[r] - xhi) / L) == m) && (xlo >= xt[r] - band) && (xhi <= xt[r] + band);
+        }
+        if (__syncthreads_and(simple)) {
+            const double sl = range_sum(pl, nd.m0, nd.m1 + 1), slx = range_sum(plx, nd.m0, nd.m1 + 1);
+#pragma unroll
+            for (int r = 0; r < kNearR; ++r) exact[r] -= cbg * (xt[r] * sl - slx);
+            const float2 e2v = make_float2(eps2, eps2);
+            for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile) {
+                const int cnt = min(kNearTile, nd.m1 - t0 + 1);
+                const double base = sx[t0];
+                __syncthreads();
+                for (int k = threadIdx.x; k < cnt; k += kNearThreads)
+                    shb[k] = make_float2((float)(sx[t0 + k] - base), (float)(0.5 * lam[t0 + k]));
+                __syncthreads();
+                float2 tau2[kNearR / 2], acc2[kNearR / 2], cmp2[kNearR / 2];
+#pragma unroll
+                for (int h = 0; h < kNearR / 2; ++h) {
+                    tau2[h] = make_float2((float)(xt[2 * h] - base), (float)(xt[2 * h + 1] - base));
+                    acc2[h] = make_float2(0.f, 0.f);
+                    cmp2[h] = make_float2(0.f, 0.f);
                 }
-                e = lo;
+#pragma unroll 2
+                for (int k = 0; k < cnt; ++k) {
+                    const float2 e = shb[k];
+                    const float2 nsx = make_float2(-e.x, -e.x);
+                    const float2 qh = make_float2(e.y, e.y);
+#pragma unroll
+                    for (int h = 0; h < kNearR / 2; ++h) {
+                        const float2 d = __fadd2_rn(tau2[h], nsx);
+                        const float2 r2 = __ffma2_rn(d, d, e2v);
+                        const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                        const float2 g = __fmul2_rn(d, y);
+                        const float2 v = __ffma2_rn(qh, g, make_float2(-cmp2[h].x, -cmp2[h].y));
+                        const float2 sum = __fadd2_rn(acc2[h], v);
+                        const float2 t = __fadd2_rn(sum, make_float2(-acc2[h].x, -acc2[h].y));
+                        cmp2[h] = __fadd2_rn(t, make_float2(-v.x, -v.y));
+                        acc2[h] = sum;
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < kNearR / 2; ++h) {
+                    fp[2 * h] += (double)acc2[h].x - (double)cmp2[h].x;
+                    fp[2 * h + 1] += (double)acc2[h].y - (double)cmp2[h].y;
+                }
             }
-            const int U1 = lower_bound_d(sx, a, e, xt - band);
-            int U2 = U1;
-            while (U2 < e && sx[U2] <= xt + band) ++U2;  // band holds few sources
-            exact += 0.5 * (range_sum(pl, a, U1) - range_sum(pl, U2, e)) -
-                     cbg * (xt * range_sum(pl, a, e) - range_sum(plx, a, e));
-            im[nim].xt = xt;
-            im[nim].start = a;
-            im[nim].U1 = U1;
-            im[nim].U2 = U2;
-            ++nim;
-            a = e;
-        }
-        if (a <= nd.m1) atomicCAS(err, 0, (int)FS_ERR_TREE);
-        for (int k = nim; k < 3; ++k) {
-            im[k].xt = im[nim - 1].xt;
-            im[k].start = INT_MAX;
-            im[k].U1 = im[k].U2 = 0;
-        }
-        for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile) {
-            const int cnt = min(kNearTile, nd.m1 - t0 + 1);
-            const double base = sx[t0];
-            __syncthreads();
-            for (int k = threadIdx.x; k < cnt; k += kNearThreads) {
-                const float lh = (float)(0.5 * lam[t0 + k]);
-                sh[k] = make_float4((float)(sx[t0 + k] - base), lh, lh * a1, lh * a2);
-            }
-            __syncthreads();
-            const float tau0 = (float)(im[0].xt - base), tau1 = (float)(im[1].xt - base),
-                        tau2 = (float)(im[2].xt - base);
-            const int s1 = im[1].start, s2 = im[2].start;
-            const int u10 = im[0].U1, u11 = im[1].U1, u12 = im[2].U1;
-            const int u20 = im[0].U2, u21 = im[1].U2, u22 = im[2].U2;
-            float acc = 0.f, cmp = 0.f;
-            for (int k = 0; k < cnt; ++k) {
-                const int jj = t0 + k;
-                const bool g1 = jj >= s1, g2 = jj >= s2;
-                const float tr = g2 ? tau2 : (g1 ? tau1 : tau0);
-                const int U1 = g2 ? u12 : (g1 ? u11 : u10);
-                const int U2 = g2 ? u22 : (g1 ? u21 : u20);
-                const float4 e = sh[k];
-                const float d = tr - e.x;
-                const float y = rsqrtf(fmaf(d, d, eps2));
-                const float z = y * y;
-                const float c = z * fmaf(z, e.w, e.z);
-                const float v = (jj < U1) ? -c : ((jj >= U2) ? c : e.y * (d * y));
-                const float w = v - cmp;
-                const float t = acc + w;
-                cmp = (t - acc) - w;
-                acc = t;
-            }
-            fp += (double)acc - (double)cmp;
+        } else {
+#pragma unroll 1
+            for (int r = 0; r < kNearR; ++r)
+                near_general(nd, x[r], sx, lam, pl, plx, L, band, cbg, eps2, a1, a2, shg, exact[r], fp[r], err);
         }
     }
-    if (active) apply_stage(S, sidx[j], efar[j] + norm * (exact + fp));
+#pragma unroll
+    for (int r = 0; r < kNearR; ++r)
+        if (jt[r] <= leaf.m1) apply_stage(S, sidx[jt[r]], efar[jt[r]] + norm * (exact[r] + fp[r]));
 }
 
 __global__ void k_mul(const double* __restrict__ a, const double* __restrict__ b, int n, double* __restrict__ c) {
@@ -682,8 +768,8 @@ class Treecode final : public FieldEngine {
                 k_far32<<<(n + 127) / 128, 128, 0, st>>>(nodes_.p, meta_.p, leaf_of_.p, far_.p, far_n_.p, mom_.p,
                                                         consts_.p, sx_.p, n, P_, L_, eps_, norm_, cbg_, efar_.p);
             }
-            // leaves hold < max_source points: at most ceil(max_source/256) target blocks each
-            dim3 grid(cap_leaves, (N0_ + kNearThreads - 1) / kNearThreads);
+            // leaves hold < max_source points: at most ceil(max_source/kNearBlock) target blocks each
+            dim3 grid(cap_leaves, (N0_ + kNearBlock - 1) / kNearBlock);
             size_t tb2 = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb2, lam_.p, pl_.p, n, st));
             k_mul<<<(n + T - 1) / T, T, 0, st>>>(lam_.p, sx_.p, n, lx_.p);
