@@ -39,12 +39,15 @@ typedef enum fs_status {
 /* Field solver kind.  DIRECT64 is the reference arithmetic in FP64 (bit-exact
  * with E_MQ_DirectSum); DIRECT32C is the FP32 pair kernel with compensation and
  * FP64 background; TREECODE64 / TREECODE32C are the barycentric Lagrange
- * treecode of E_MQ_Treecode with an FP64 / FP32-compensated near field. */
+ * treecode of E_MQ_Treecode with an FP64 / FP32-compensated near field;
+ * DIRECT64_OPEN is E_MQ_DirectSum_openbcs (src/FieldStructure.cpp:170-192),
+ * open boundaries, bit-exact, field plugin only (L is ignored). */
 typedef enum fs_field_kind {
     FS_FIELD_DIRECT64 = 0,
     FS_FIELD_DIRECT32C = 1,
     FS_FIELD_TREECODE64 = 2,
-    FS_FIELD_TREECODE32C = 3
+    FS_FIELD_TREECODE32C = 3,
+    FS_FIELD_DIRECT64_OPEN = 4
 } fs_field_kind;
 
 /* Parameters of AMRSimulation::make_field_return_ptr
@@ -118,6 +121,12 @@ typedef struct fs_sim_params {
     int num_species;              /* 1..8                                       */
     fs_species_params species[8];
     int device;
+    /* Drive field added to E at every evaluation, at the evaluation's time
+     * (deck "external_field", AMRSimulation_load.cpp:98-136; ExternalTanh /
+     * ExternalSine / ExternalLogistic, src/FieldStructure.cpp:15-96). */
+    int use_external_field;       /* 0 off                                      */
+    int external_type;            /* 0 tanh, 1 sine, 2 logistic                 */
+    double external_Am, external_k, external_omega;
 } fs_sim_params;
 
 typedef struct fs_sim fs_sim;

@@ -28,6 +28,7 @@ FS_FIELD_DIRECT64 = 0
 FS_FIELD_DIRECT32C = 1
 FS_FIELD_TREECODE64 = 2
 FS_FIELD_TREECODE32C = 3
+FS_FIELD_DIRECT64_OPEN = 4
 PANEL_INTS = 18
 
 STATUS = {0: "FS_OK", 1: "FS_ERR_ARG", 2: "FS_ERR_CUDA", 3: "FS_ERR_NOMEM", 4: "FS_ERR_WALK",
@@ -67,7 +68,9 @@ class SimParams(C.Structure):
     _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("quadrature", C.c_int), ("dt", C.c_double),
                 ("remesh_period", C.c_int), ("greens_epsilon", C.c_double), ("field_kind", C.c_int),
                 ("mac", C.c_double), ("degree", C.c_int), ("max_source", C.c_int), ("num_species", C.c_int),
-                ("species", SpeciesParams * 8), ("device", C.c_int)]
+                ("species", SpeciesParams * 8), ("device", C.c_int), ("use_external_field", C.c_int),
+                ("external_type", C.c_int), ("external_Am", C.c_double), ("external_k", C.c_double),
+                ("external_omega", C.c_double)]
 
 
 class PoolParams(C.Structure):
@@ -259,6 +262,14 @@ class E_MQ_DirectSum_B200(_Field):
         super().__init__(L, epsilon, kind, device=device)
 
 
+class E_MQ_DirectSum_openbcs_B200(_Field):
+    """E_MQ_DirectSum_openbcs(epsilon) (src/FieldStructure.cpp:166-192) on the
+    GPU: open boundaries, FP64, bit-identical to the reference."""
+
+    def __init__(self, epsilon, device=0):
+        super().__init__(1.0, epsilon, FS_FIELD_DIRECT64_OPEN, device=device)
+
+
 class E_MQ_Treecode_B200(_Field):
     """E_MQ_Treecode(L, epsilon, mac, degree, max_source, max_target, verbosity)
     (src/FieldStructure.cpp:210-503) on the GPU.  Like the reference it ignores
@@ -279,7 +290,7 @@ def field_eval_noalloc(L, epsilon, d_es, d_x, d_q_ws, n, stream=None):
 
 # --------------------------------------------------------------------- simulation
 FIELD_KINDS = {"direct64": FS_FIELD_DIRECT64, "direct32c": FS_FIELD_DIRECT32C, "treecode64": FS_FIELD_TREECODE64,
-               "treecode32c": FS_FIELD_TREECODE32C}
+               "treecode32c": FS_FIELD_TREECODE32C, "direct64_open": FS_FIELD_DIRECT64_OPEN}
 
 
 def sim_params(deck: dict, field_backend: str | None = None, device: int = 0) -> SimParams:
@@ -314,6 +325,12 @@ def sim_params(deck: dict, field_backend: str | None = None, device: int = 0) ->
         S.pth, S.pstr, S.amp = float(sp.get("pth", 1.0)), float(sp.get("pstr", 0.0)), float(sp.get("amp", 0.0))
         S.normalized_wavenumber = float(sp.get("normalized_wavenumber", 1.0))
     P.device = int(device)
+    # "external_field" block (AMRSimulation_load.cpp:98-136); absent = off
+    ext = deck.get("external_field") or {}
+    if int(ext.get("use_external_field", 0)) > 0:
+        P.use_external_field = 1
+        P.external_type = int(ext.get("external_type", 0))
+        P.external_Am, P.external_k, P.external_omega = float(ext["Am"]), float(ext["k"]), float(ext["omega"])
     return P
 
 

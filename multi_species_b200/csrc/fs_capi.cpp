@@ -57,13 +57,15 @@ fs_status fs_field_create(const fs_field_params* params, fs_field** out) {
     auto* f = new fs_field();
     fs_status rc = fsb::guard([&] {
         const fs_field_params& P = *params;
-        if (!(P.L > 0) || !(P.epsilon > 0)) fsb::fail(FS_ERR_ARG, "L and epsilon must be positive");
+        if (!(P.epsilon > 0)) fsb::fail(FS_ERR_ARG, "epsilon must be positive");
+        if (P.kind != FS_FIELD_DIRECT64_OPEN && !(P.L > 0)) fsb::fail(FS_ERR_ARG, "L must be positive");
         f->prm = P;
         FS_CUDA(cudaSetDevice(P.device));
         FS_CUDA(cudaStreamCreateWithFlags(&f->st, cudaStreamNonBlocking));
         switch (P.kind) {
             case FS_FIELD_DIRECT64: f->engine.reset(fsb::make_direct64(P.L, P.epsilon)); break;
             case FS_FIELD_DIRECT32C: f->engine.reset(fsb::make_direct32c(P.L, P.epsilon)); break;
+            case FS_FIELD_DIRECT64_OPEN: f->engine.reset(fsb::make_direct64_open(P.epsilon)); break;
             case FS_FIELD_TREECODE64:
             case FS_FIELD_TREECODE32C:
                 if (P.degree < 1 || P.degree > 16) fsb::fail(FS_ERR_ARG, "treecode degree must be 1..16");

@@ -28,6 +28,9 @@ __device__ __forceinline__ double stage_qm(const Stage& S, int o) {
 // RK4 epilogue for point o given the raw field E at that point
 // (src/simulation_files/AMRSimulation_step.cpp:178-248).
 __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
+    // evaluate_field (AMRSimulation_field.cpp:164-173): the drive field is
+    // added to the field before the stage uses it, es += a sin(k x - omega t)
+    if (S.ext_x) E = dadd(E, dmul(S.ext_a, sin(dsub(dmul(S.ext_k, S.ext_x[o]), S.ext_omt))));
     switch (S.kind) {
         case STAGE_STORE:
             S.out[o] = E;

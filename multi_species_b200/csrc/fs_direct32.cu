@@ -209,7 +209,10 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // (2e-9 of the pair's q/2) and falls off as 1/d^6.  Far pairs need no square
 // root and one FMA for the series, and two targets share one MUFU.RCP:
 // w'_a = r_b / (r_a r_b).
-constexpr double kBand = 16.0;
+#ifndef FS_PAIR_BAND
+#define FS_PAIR_BAND 16.0
+#endif
+constexpr double kBand = FS_PAIR_BAND;  // near band half-width in units of eps
 constexpr int kMaxChunks = 64;
 
 // One (target block, source chunk) of a job: kR targets per thread, the

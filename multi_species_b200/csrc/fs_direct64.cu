@@ -50,6 +50,51 @@ k_direct64(const double* __restrict__ tx, int nt, const double* __restrict__ sx,
     if (i < nt) apply_stage(S, i, ei);
 }
 
+// Open boundaries, E_MQ_DirectSum_openbcs::operator() (src/FieldStructure.cpp:170-192):
+// es_i = sum_j ((q_j * 0.5) * z) / sqrt(z*z + eps^2) - x_i, z = x_i - x_j, in the
+// reference's order and roundings (bit-identical).
+__global__ void __launch_bounds__(kThreads64)
+k_direct64_open(const double* __restrict__ tx, int nt, const double* __restrict__ sx, const double* __restrict__ sq,
+                int ns, double eps, Stage S) {
+    __shared__ double sh_x[kTile64];
+    __shared__ double sh_q[kTile64];
+    const int i = blockIdx.x * kThreads64 + threadIdx.x;
+    const double xi = (i < nt) ? tx[i] : 0.0;
+    const double eps_sq = dmul(eps, eps);
+    double ei = 0.0;
+    for (int base = 0; base < ns; base += kTile64) {
+        const int cnt = min(kTile64, ns - base);
+        for (int k = threadIdx.x; k < cnt; k += kThreads64) {
+            sh_x[k] = sx[base + k];
+            sh_q[k] = sq[base + k];
+        }
+        __syncthreads();
+        for (int j = 0; j < cnt; ++j) {
+            const double z = dsub(xi, sh_x[j]);
+            ei = dadd(ei, ddiv(dmul(dmul(sh_q[j], 0.5), z), __dsqrt_rn(dadd(dmul(z, z), eps_sq))));
+        }
+        __syncthreads();
+    }
+    if (i < nt) apply_stage(S, i, dsub(ei, xi));
+}
+
+class Direct64Open final : public FieldEngine {
+   public:
+    explicit Direct64Open(double eps) : eps_(eps) {}
+    void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
+              cudaStream_t st) override {
+        last_pairs = (double)nt * (double)ns;
+        if (nt <= 0) return;
+        const int blocks = (nt + kThreads64 - 1) / kThreads64;
+        ProfScope prof("k_direct64_open", st, last_pairs);
+        k_direct64_open<<<blocks, kThreads64, 0, st>>>(d_t, nt, d_s, d_q, ns, eps_, stage);
+        FS_LAUNCHED(1);
+    }
+
+   private:
+    double eps_;
+};
+
 class Direct64 final : public FieldEngine {
    public:
     Direct64(double L, double eps) : L_(L), eps_(eps) {
@@ -73,5 +118,6 @@ class Direct64 final : public FieldEngine {
 }  // namespace
 
 FieldEngine* make_direct64(double L, double eps) { return new Direct64(L, eps); }
+FieldEngine* make_direct64_open(double eps) { return new Direct64Open(eps); }
 
 }  // namespace fsb

@@ -125,6 +125,10 @@ struct Stage {
     int nsp = 1;
     int start[9] = {0};
     double qm[8] = {0};
+    // drive field: E += ext_a * sin(ext_k * ext_x[o] - ext_omt) when ext_x is set
+    // (ext_x = the evaluation's targets, in the caller's order)
+    const double* ext_x = nullptr;
+    double ext_a = 0, ext_k = 0, ext_omt = 0;
 };
 
 // ------------------------------------------------------------------ host mesh
@@ -219,6 +223,7 @@ int pairs_batched_grid(int R);
 void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost);
 
 FieldEngine* make_direct64(double L, double eps);
+FieldEngine* make_direct64_open(double eps);
 FieldEngine* make_direct32c(double L, double eps);
 FieldEngine* make_treecode(double L, double eps, double mac, int degree, int max_source, bool fp32_near);
 

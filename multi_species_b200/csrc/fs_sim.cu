@@ -519,6 +519,28 @@ struct SpeciesState {
     DevBuf<int> inv, col_off, col_idx;
 };
 
+// Drive-field amplitude at time t (src/FieldStructure.cpp:15-96): ExternalTanh
+// (type 0, its factor k included) switches on around t = 69 and off around
+// t = 307 with widths 20, normalised to start from zero at t = 0; ExternalSine
+// (1) ramps up to t = 50, holds to 150 and ramps down to 200; ExternalLogistic
+// (2) switches on at t = 10 and off at t = 110.  Host double arithmetic in the
+// reference's expression order.
+double tanh_switch(double t) { return 0.5 * (std::tanh((t - 69.0) / 20.0) - std::tanh((t - 307.0) / 20.0)); }
+double drive_amplitude(int type, double Am, double k, double t) {
+    if (type == 1) {
+        if (t < 50.0) return Am * std::sin(t * M_PI / 100);
+        if (t < 150.0) return Am;
+        if (t < 200.0) return Am * std::cos((t - 150) * M_PI / 100);
+        return 0.0;
+    }
+    if (type == 2) {
+        if (t < 60.0) return Am / (1.0 + std::exp(-40.0 * (t - 10.0)));
+        return Am * (1.0 - 1.0 / (1.0 + std::exp(-40.0 * (t - 110.0))));
+    }
+    const double e0 = tanh_switch(0.0);
+    return (tanh_switch(t) - e0) / (1 - e0) * Am * k;
+}
+
 struct Sim {
     fs_sim_params prm{};
     int N = 0, U = 0, iter = 0;
@@ -563,6 +585,10 @@ struct Sim {
         if (P.num_species < 1 || P.num_species > 8) fail(FS_ERR_ARG, "num_species must be 1..8");
         if (!(P.xmax > P.xmin)) fail(FS_ERR_ARG, "xmax must exceed xmin");
         if (P.remesh_period < 1) fail(FS_ERR_ARG, "remesh_period must be >= 1");
+        if (P.field_kind == FS_FIELD_DIRECT64_OPEN)
+            fail(FS_ERR_UNSUPPORTED, "open boundaries are supported by the field plugin only, not by the session");
+        if (P.use_external_field && (P.external_type < 0 || P.external_type > 2))
+            fail(FS_ERR_ARG, "external_type must be 0 (tanh), 1 (sine) or 2 (logistic)");
         FS_CUDA(cudaSetDevice(P.device));
         if (external) {
             st = external;
@@ -750,11 +776,22 @@ struct Sim {
         }
         FS_LAUNCHED((long long)sp.size());
     }
+    // The drive field at time tc on the call's targets (evaluate_field and
+    // evaluate_field_uniform_grid add it after the field).
+    FieldCall with_drive(FieldCall fc, double tc) const {
+        if (prm.use_external_field) {
+            fc.stage.ext_x = fc.x;
+            fc.stage.ext_a = drive_amplitude(prm.external_type, prm.external_Am, prm.external_k, tc);
+            fc.stage.ext_k = prm.external_k;
+            fc.stage.ext_omt = prm.external_omega * tc;
+        }
+        return fc;
+    }
     FieldCall reduced_call() const {
         Stage S = base;
         S.kind = STAGE_STORE;
         S.out = re.p;
-        return FieldCall{rx.p, U, rw.p, S};
+        return with_drive(FieldCall{rx.p, U, rw.p, S}, t);
     }
     void reduced_post() {
         for (auto& s : sp) {
@@ -841,17 +878,21 @@ struct Sim {
             }
         }
     }
+    // Stage times of rk4_step (AMRSimulation_step.cpp:170, :201, :224):
+    // t2 = t + dt/2 for the second and third stages, t + dt for the fourth;
+    // the end-of-step evaluation and the remesh use the advanced t (:84-89).
     FieldCall call(int c) const {
+        const double t2 = t + prm.dt * 0.5, t4 = t + prm.dt;
         switch (c) {
-            case 0: return FieldCall{xkA.p, N, qw.p, stage(STAGE_RK2, xkB.p)};
-            case 1: return FieldCall{xkB.p, N, qw.p, stage(STAGE_RK3, xkA.p)};
-            case 2: return FieldCall{xkA.p, N, qw.p, stage(STAGE_RK4, nullptr)};
+            case 0: return with_drive(FieldCall{xkA.p, N, qw.p, stage(STAGE_RK2, xkB.p)}, t2);
+            case 1: return with_drive(FieldCall{xkB.p, N, qw.p, stage(STAGE_RK3, xkA.p)}, t2);
+            case 2: return with_drive(FieldCall{xkA.p, N, qw.p, stage(STAGE_RK4, nullptr)}, t4);
             default: {
                 if (remeshing) return reduced_call();
                 Stage S = base;
                 S.kind = STAGE_STORE;
                 S.out = e.p;
-                return FieldCall{x.p, N, qw.p, S};
+                return with_drive(FieldCall{x.p, N, qw.p, S}, t);
             }
         }
     }
@@ -1301,9 +1342,13 @@ struct Batch {
         for (auto& s : sims) s->check_status();
     }
 
+    // Captured kernels keep their arguments: members whose drive field changes
+    // with time, or whose field kind synchronises with the host, step launch by launch.
     bool graphable() const {
-        for (auto& s : sims)
+        for (auto& s : sims) {
             if (s->prm.field_kind != FS_FIELD_DIRECT32C && s->prm.field_kind != FS_FIELD_DIRECT64) return false;
+            if (s->prm.use_external_field) return false;
+        }
         return true;
     }
 

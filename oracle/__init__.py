@@ -50,7 +50,9 @@ class FsoSim(C.Structure):
     _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("quadrature", C.c_int),
                 ("dt", C.c_double), ("remesh_period", C.c_int), ("greens_epsilon", C.c_double),
                 ("use_treecode", C.c_int), ("mac", C.c_double), ("degree", C.c_int),
-                ("max_source", C.c_int), ("num_species", C.c_int), ("species", FsoSpecies * 8)]
+                ("max_source", C.c_int), ("num_species", C.c_int), ("species", FsoSpecies * 8),
+                ("use_external_field", C.c_int), ("external_type", C.c_int), ("ext_Am", C.c_double),
+                ("ext_k", C.c_double), ("ext_omega", C.c_double)]
 
 
 _lib = None
@@ -82,6 +84,11 @@ def lib():
         L.fso_remesh_interp.restype = C.c_int
         L.fso_reduce.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _ip]
         L.fso_reduce.restype = C.c_int
+        L.fso_direct_sum_open.argtypes = [C.c_double, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        L.fso_external_amplitude.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+        L.fso_external_amplitude.restype = C.c_double
+        L.fso_external_field.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, C.c_int,
+                                         C.c_double]
         L.fso_sim_create.argtypes = [C.POINTER(FsoSim)]
         L.fso_sim_create.restype = C.c_void_p
         L.fso_sim_destroy.argtypes = [C.c_void_p]
@@ -114,6 +121,10 @@ def ref():
         R.fsref_set_threads.restype = C.c_int
         R.fsref_direct_sum.argtypes = [C.c_double, C.c_double, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
         R.fsref_direct_sum.restype = C.c_int
+        R.fsref_direct_sum_open.argtypes = [C.c_double, _dp, _dp, C.c_int, _dp, _dp, C.c_int]
+        R.fsref_direct_sum_open.restype = C.c_int
+        R.fsref_external.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, C.c_int, C.c_double]
+        R.fsref_external.restype = C.c_int
         R.fsref_treecode.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                      _dp, _dp, C.c_int, _dp, _dp, C.c_int]
         R.fsref_treecode.restype = C.c_int
@@ -130,6 +141,35 @@ def direct_sum(L, eps, targets, sources, q):
     t, s, q = _f64(targets), _f64(sources), _f64(q)
     es = np.zeros(len(t))
     lib().fso_direct_sum(L, eps, es, t, len(t), s, q, len(s))
+    return es
+
+
+def direct_sum_open(eps, targets, sources, q):
+    """E_MQ_DirectSum_openbcs (src/FieldStructure.cpp:170-192), restated."""
+    t, s, q = _f64(targets), _f64(sources), _f64(q)
+    es = np.zeros(len(t))
+    lib().fso_direct_sum_open(eps, es, t, len(t), s, q, len(s))
+    return es
+
+
+def external_field(kind, Am, k, omega, es, x, t):
+    """Drive field added into es in place (src/FieldStructure.cpp:15-96), restated;
+    kind 0 tanh, 1 sine, 2 logistic."""
+    x = _f64(x)
+    lib().fso_external_field(int(kind), Am, k, omega, es, x, len(x), t)
+    return es
+
+
+def ref_direct_sum_open(eps, targets, sources, q):
+    t, s, q = _f64(targets), _f64(sources), _f64(q)
+    es = np.zeros(len(t))
+    ref().fsref_direct_sum_open(eps, es, t, len(t), s, q, len(s))
+    return es
+
+
+def ref_external_field(kind, Am, k, omega, es, x, t):
+    x = _f64(x)
+    ref().fsref_external(int(kind), Am, k, omega, es, x, len(x), t)
     return es
 
 
@@ -236,6 +276,11 @@ def sim_params(deck: dict) -> FsoSim:
         S.ics_type = int(sp.get("ics_type", 1))
         S.pth, S.pstr, S.amp = sp.get("pth", 1.0), sp.get("pstr", 0.0), sp.get("amp", 0.0)
         S.normalized_wavenumber = sp.get("normalized_wavenumber", 1.0)
+    ext = deck.get("external_field") or {}
+    P.use_external_field = 1 if int(ext.get("use_external_field", 0)) > 0 else 0
+    if P.use_external_field:
+        P.external_type = int(ext.get("external_type", 0))
+        P.ext_Am, P.ext_k, P.ext_omega = float(ext["Am"]), float(ext["k"]), float(ext["omega"])
     return P
 
 

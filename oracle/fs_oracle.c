@@ -907,6 +907,50 @@ int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old
 }
 
 /* ======================================================================= */
+/* Open-boundary direct sum and drive fields                                */
+/* ======================================================================= */
+void fso_direct_sum_open(double eps, double* es, const double* targets, int nt, const double* sources,
+                         const double* q_ws, int ns) {
+    const double e2 = eps * eps;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nt; ++i) {
+        const double x = targets[i];
+        double acc = 0.0;
+        for (int j = 0; j < ns; ++j) {
+            const double z = x - sources[j];
+            acc += q_ws[j] * 0.5 * z / sqrt(z * z + e2);
+        }
+        es[i] = acc - x;
+    }
+}
+
+/* ExternalTanh switches on around t = 69 and off around t = 307 (widths 20),
+ * normalised so that it starts from zero at t = 0 (FieldStructure.cpp:17-36). */
+static double tanh_switch(double t) { return 0.5 * (tanh((t - 69.0) / 20.0) - tanh((t - 307.0) / 20.0)); }
+
+double fso_external_amplitude(int type, double Am, double k, double t) {
+    if (type == 1) {  /* ExternalSine (:48-64): ramp up to t=50, hold to 150, ramp down to 200 */
+        if (t < 50.0) return Am * sin(t * M_PI / 100);
+        if (t < 150.0) return Am;
+        if (t < 200.0) return Am * cos((t - 150) * M_PI / 100);
+        return 0.0;
+    }
+    if (type == 2) {  /* ExternalLogistic (:70-84): logistic on at t=10, off at t=110 */
+        if (t < 60.0) return Am / (1.0 + exp(-40.0 * (t - 10.0)));
+        return Am * (1.0 - 1.0 / (1.0 + exp(-40.0 * (t - 110.0))));
+    }
+    const double e0 = tanh_switch(0.0);
+    return (tanh_switch(t) - e0) / (1 - e0) * Am * k;
+}
+
+void fso_external_field(int type, double Am, double k, double omega, double* es, const double* x, int n,
+                        double t) {
+    const double a = fso_external_amplitude(type, Am, k, t);
+    const double omt = omega * t;
+    for (int i = 0; i < n; ++i) es[i] += a * sin(k * x[i] - omt);
+}
+
+/* ======================================================================= */
 /* Reduced grid                                                             */
 /* ======================================================================= */
 static const double* g_rx;
@@ -952,10 +996,14 @@ struct fso_sim {
     long long full_evals, reduced_evals;
 };
 
-static void sim_field(fso_sim* s, double* es, const double* x, const double* q, int n) {
+/* evaluate_field (AMRSimulation_field.cpp:164-173): the field, then the drive
+ * field at time t on the same positions. */
+static void sim_field(fso_sim* s, double* es, const double* x, const double* q, int n, double t) {
     const fso_sim_params* P = &s->prm;
     if (P->use_treecode) fso_treecode(s->Lx, P->greens_epsilon, P->mac, P->degree, P->max_source, es, x, q, n);
     else fso_direct_sum(s->Lx, P->greens_epsilon, es, x, n, x, q, n);
+    if (P->use_external_field)
+        fso_external_field(P->external_type, P->ext_Am, P->ext_k, P->ext_omega, es, x, n, t);
 }
 
 /* evaluate_field_uniform_grid (src/simulation_files/AMRSimulation_field.cpp:5-162). */
@@ -973,7 +1021,7 @@ static void sim_reduced_field(fso_sim* s) {
     }
     off[ns] = tot;
     double* re = (double*)malloc(sizeof(double) * tot);
-    sim_field(s, re, rx, rw, tot);
+    sim_field(s, re, rx, rw, tot, s->t);
     s->reduced_evals++;
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) s->es[i] = re[off[sp] + inv[i]];
@@ -1051,21 +1099,22 @@ static void sim_rk4(fso_sim* s) {
             p2[i] = s->ps[i] + 0.5 * dt * e1[i];
             xk[i] = s->xs[i] + 0.5 * dt * p1[i];
         }
-    sim_field(s, e2, xk, s->qws, N);
+    const double t2 = s->t + dt * 0.5, t4 = s->t + dt;  /* rk4_step :170, :201, :224 */
+    sim_field(s, e2, xk, s->qws, N, t2);
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
             e2[i] *= s->qm[sp];
             p3[i] = s->ps[i] + 0.5 * dt * e2[i];
             xk[i] = s->xs[i] + 0.5 * dt * p2[i];
         }
-    sim_field(s, e3, xk, s->qws, N);
+    sim_field(s, e3, xk, s->qws, N, t2);
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
             e3[i] *= s->qm[sp];
             p4[i] = s->ps[i] + dt * e3[i];
             xk[i] = s->xs[i] + dt * p3[i];
         }
-    sim_field(s, e4, xk, s->qws, N);
+    sim_field(s, e4, xk, s->qws, N, t4);
     s->full_evals += 3;
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) e4[i] *= s->qm[sp];
@@ -1102,7 +1151,7 @@ int fso_sim_step(fso_sim* s) {
     s->iter += 1;
     s->t += s->prm.dt;
     if (s->iter % s->prm.remesh_period == 0) return sim_remesh(s);
-    sim_field(s, s->es, s->xs, s->qws, s->N);
+    sim_field(s, s->es, s->xs, s->qws, s->N, s->t);
     s->full_evals += 1;
     return 0;
 }

@@ -79,6 +79,18 @@ void fso_panel_fit(const double* px, const double* py, const double* pf, int npt
 int fso_reduce(const double* xs, const double* q_ws, int n, double* reduced_xs,
                double* reduced_ws, int* inv);
 
+/* E_MQ_DirectSum_openbcs::operator() (src/FieldStructure.cpp:170-192):
+ * open boundaries, es[i] = sum_j q_j 0.5 z / sqrt(z^2 + eps^2) - x_i. */
+void fso_direct_sum_open(double eps, double* es, const double* targets, int nt, const double* sources,
+                         const double* q_ws, int ns);
+
+/* Drive fields (src/FieldStructure.cpp:15-96): amplitude at time t of
+ * ExternalTanh (type 0, including its factor k), ExternalSine (1) and
+ * ExternalLogistic (2); fso_external_field adds amp * sin(k x - omega t). */
+double fso_external_amplitude(int type, double Am, double k, double t);
+void fso_external_field(int type, double Am, double k, double omega, double* es, const double* x, int n,
+                        double t);
+
 /* ---------------- simulation ---------------- */
 typedef struct {
     double q, m;
@@ -100,6 +112,10 @@ typedef struct {
     int max_source;
     int num_species;
     fso_species_params species[8];
+    /* deck "external_field" (AMRSimulation_load.cpp:98-136) */
+    int use_external_field;
+    int external_type;   /* 0 tanh, 1 sine, 2 logistic */
+    double ext_Am, ext_k, ext_omega;
 } fso_sim_params;
 
 typedef struct fso_sim fso_sim;

@@ -144,4 +144,34 @@ int fsref_treecode(double L, double epsilon, double mac, int degree, int max_sou
     return 0;
 }
 
+// E_MQ_DirectSum_openbcs(epsilon)(es, targets, nt, sources, q_ws, ns)
+//   (src/FieldStructure.cpp:166-192).
+int fsref_direct_sum_open(double epsilon, double* es, const double* targets, int nt, const double* sources,
+                          const double* q_ws, int ns) {
+    CallScope scope;
+    std::vector<double> t(targets, targets + nt), s(sources, sources + ns), q(q_ws, q_ws + ns);
+    E_MQ_DirectSum_openbcs field(epsilon);
+    field(es, t.data(), nt, s.data(), q.data(), ns);
+    return 0;
+}
+
+// ExternalTanh / ExternalSine / ExternalLogistic (Am, k, omega) (es, targets, nt, t)
+//   (src/FieldStructure.cpp:15-96): adds the drive field into es.
+int fsref_external(int type, double Am, double k, double omega, double* es, const double* targets, int nt,
+                   double t) {
+    CallScope scope;
+    std::vector<double> x(targets, targets + nt);
+    if (type == 1) {
+        ExternalSine f(Am, k, omega);
+        f(es, x.data(), nt, t);
+    } else if (type == 2) {
+        ExternalLogistic f(Am, k, omega);
+        f(es, x.data(), nt, t);
+    } else {
+        ExternalTanh f(Am, k, omega);
+        f(es, x.data(), nt, t);
+    }
+    return 0;
+}
+
 }  // extern "C"

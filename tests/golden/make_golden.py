@@ -2,9 +2,11 @@
 
     python tests/golden/make_golden.py
 
-field_*.npz -- inputs and outputs of the REFERENCE's own E_MQ_DirectSum and
-    E_MQ_Treecode (src/FieldStructure.cpp), run through oracle/_ref/libfs_ref.so
-    (built from the reference sources by oracle/Makefile).  These pin the field.
+field_*.npz, drive_fields.npz -- inputs and outputs of the REFERENCE's own
+    E_MQ_DirectSum, E_MQ_DirectSum_openbcs, E_MQ_Treecode and drive fields
+    (ExternalTanh / ExternalSine / ExternalLogistic) (src/FieldStructure.cpp),
+    run through oracle/_ref/libfs_ref.so (built from the reference sources by
+    oracle/Makefile).  These pin the field.
 sim_landau_h3.npz -- a short two-species trajectory (3 panels deep, 6 steps,
     one remesh) of the C oracle restatement (oracle/liboracle.so).  The
     reference's simulation driver cannot be compiled here, so this fixture
@@ -52,6 +54,25 @@ def main():
         e = O.ref_direct_sum(c["L"], c["eps"], c["targets"], c["sources"], c["q"])
         np.savez_compressed(os.path.join(HERE, f"field_direct_{name}.npz"), L=c["L"], eps=c["eps"],
                             targets=c["targets"], sources=c["sources"], q=c["q"], es=e)
+    # open boundaries (E_MQ_DirectSum_openbcs): separate targets, coincident points
+    rng = np.random.default_rng(11)
+    src = rng.uniform(-3.0, 9.0, 600)
+    tgt = np.concatenate([rng.uniform(-4.0, 10.0, 250), src[:25]])
+    qo = rng.normal(size=600) * 1e-3
+    e = O.ref_direct_sum_open(0.05, tgt, src, qo)
+    np.savez_compressed(os.path.join(HERE, "field_open.npz"), eps=0.05, targets=tgt, sources=src, q=qo, es=e)
+    # drive fields (ExternalTanh / Sine / Logistic) at times across their switches
+    x = rng.uniform(-5.0, 30.0, 200)
+    times = np.array([0.0, 3.0, 9.75, 10.0, 49.0, 60.0, 70.0, 120.0, 175.0, 205.0, 300.0])
+    drive = {}
+    for kind in (0, 1, 2):
+        out = []
+        for t in times:
+            e0 = np.zeros_like(x)
+            out.append(O.ref_external_field(kind, 0.3, 0.26, 0.37, e0, x, float(t)))
+        drive[f"es_{kind}"] = np.array(out)
+    np.savez_compressed(os.path.join(HERE, "drive_fields.npz"), x=x, times=times, Am=0.3, k=0.26, omega=0.37,
+                        **drive)
     rng = np.random.default_rng(7)
     L = 20 * np.pi
     x = rng.uniform(-L / 2, 1.5 * L, 5000)

@@ -144,3 +144,19 @@ def test_treecode_rejects_distinct_targets():
     f = M.E_MQ_Treecode_B200(1.0, 0.1, 0.7, 8, 100)
     with pytest.raises(M.FsError):
         f.evaluate(np.zeros(3), np.zeros(4), np.zeros(4))
+
+
+def test_open_boundary_plugin_bit_identical_to_reference_golden():
+    g = np.load(os.path.join(GOLD, "field_open.npz"))
+    f = M.E_MQ_DirectSum_openbcs_B200(float(g["eps"]))
+    e = f.evaluate(g["targets"], g["sources"], g["q"])
+    assert np.array_equal(e, g["es"])
+
+
+@pytest.mark.parametrize("n", [1, 1000, 20000])
+def test_open_boundary_plugin_vs_oracle(n):
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-10.0, 30.0, n)
+    q = rng.normal(size=n) * 1e-3
+    f = M.E_MQ_DirectSum_openbcs_B200(0.02)
+    assert np.array_equal(f.evaluate(x, x, q), O.direct_sum_open(0.02, x, x, q))

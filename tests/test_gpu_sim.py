@@ -137,3 +137,41 @@ def test_treecode32c_simulation_field_error():
     g64.step(2)
     g32.step(2)
     assert rel(g32.state()["es"], g64.state()["es"]) < 1e-6
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_drive_field_session_matches_oracle(kind):
+    """Drive fields (tanh / sine / logistic) added at every evaluation with the
+    stage times of rk4_step; 24 steps of 0.5 cross the logistic switch-on at
+    t = 10 and include four remeshes.  The device sine differs from the host's
+    by at most an ulp, so the bound is a rounding-level one."""
+    d = decks.landau_two_species(h=3, ph=1, steps=24)
+    d["species_list"] = d["species_list"][:1]  # electrons: the cold ions of this coarse mesh tangle by step 20
+    d["external_field"] = {"use_external_field": 1, "external_type": kind, "Am": 0.4, "k": 0.5, "omega": 0.37}
+    g, o = M.Simulation(d, "direct64"), O.Sim(d)
+    for step in range(24):
+        g.step()
+        o.step()
+        a, b = g.state(), o.state()
+        for k in ("xs", "ps", "es"):
+            assert rel(a[k], b[k]) < 1e-11, (step, k)
+    d.pop("external_field")
+    und = O.Sim(d)
+    und.step(24)
+    assert rel(g.state()["es"], und.state()["es"]) > 1e-6  # the drive acted
+
+
+def test_drive_field_fp32c_session():
+    """FP32c session with a sine drive: after 3 steps its E minus the drive at
+    t = 3 dt is the FP64 field at its own positions, within the FP32c bound
+    (relative to the field: the drive is added exactly in FP64)."""
+    d = decks.two_stream(h=6, ph=1, remesh_period=5)
+    d["external_field"] = {"use_external_field": 1, "external_type": 1, "Am": 0.4, "k": 0.2, "omega": 0.37}
+    g32 = M.Simulation(d, "direct32c")
+    g32.step(3)
+    st = g32.state()
+    L = d["xmax"] - d["xmin"]
+    field = M.E_MQ_DirectSum_B200(L, d["greens_epsilon"], "fp64").evaluate(st["xs"], st["xs"], st["q_ws"])
+    drive = O.external_field(1, 0.4, 0.2, 0.37, np.zeros(len(st["xs"])), st["xs"], 3 * d["dt"])
+    assert np.max(np.abs(drive)) > 1e-3
+    assert rel(st["es"] - drive, field) < 1e-6

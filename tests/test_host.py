@@ -71,3 +71,15 @@ def test_pool_estimate_grows_with_points_and_rejects_bad_params():
     for kw in (dict(max_live=0), dict(hbm_budget=0.0), dict(tuning=(3, 8)), dict(tuning=(4, 0))):
         with pytest.raises(fs.FsError):
             fs.Pool(**kw)
+
+
+def test_session_rejects_open_boundaries_and_bad_drive():
+    from multi_species_b200 import decks
+    d = decks.landau_two_species(h=3, ph=1)
+    with pytest.raises(M.FsError) as e:
+        M.Simulation(d, "direct64_open")
+    assert e.value.code == 8  # FS_ERR_UNSUPPORTED: field plugin only
+    d2 = dict(d, external_field={"use_external_field": 1, "external_type": 7, "Am": 0.1, "k": 0.5, "omega": 0.3})
+    with pytest.raises(M.FsError) as e:
+        M.Simulation(d2)
+    assert e.value.code == 1

@@ -19,6 +19,39 @@ def test_direct_sum_matches_reference_golden_bitwise(path):
     assert np.array_equal(e, g["es"])
 
 
+def test_open_boundary_sum_matches_reference_golden_bitwise():
+    g = np.load(os.path.join(GOLD, "field_open.npz"))
+    e = O.direct_sum_open(float(g["eps"]), g["targets"], g["sources"], g["q"])
+    assert np.array_equal(e, g["es"])
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_drive_fields_match_reference_golden_bitwise(kind):
+    g = np.load(os.path.join(GOLD, "drive_fields.npz"))
+    for t, ref in zip(g["times"], g[f"es_{kind}"]):
+        e = O.external_field(kind, float(g["Am"]), float(g["k"]), float(g["omega"]), np.zeros_like(g["x"]),
+                             g["x"], float(t))
+        assert np.array_equal(e, ref), t
+
+
+def test_drive_field_in_the_session():
+    """The oracle session adds the drive at every evaluation, at the
+    evaluation's time: after a step, E is the field at the new positions plus
+    the drive at t = dt on them, and the trajectory differs from the undriven one."""
+    d = decks.landau_two_species(h=3, ph=1, steps=4)
+    d["remesh_period"] = 100
+    d2 = dict(d, external_field={"use_external_field": 1, "external_type": 1, "Am": 0.4, "k": 0.5, "omega": 0.37})
+    s0, s1 = O.Sim(d), O.Sim(d2)
+    s0.step(1)
+    s1.step(1)
+    a, b = s0.state(), s1.state()
+    assert not np.array_equal(a["xs"], b["xs"])
+    L = d["xmax"] - d["xmin"]
+    field = O.direct_sum(L, d["greens_epsilon"], b["xs"], b["xs"], b["q_ws"])
+    drive = O.external_field(1, 0.4, 0.5, 0.37, np.zeros(len(b["xs"])), b["xs"], d["dt"])
+    assert np.max(np.abs(b["es"] - field - drive)) <= 4e-16 * np.max(np.abs(field))
+
+
 def test_treecode_matches_reference_golden_bitwise():
     g = np.load(os.path.join(GOLD, "field_treecode.npz"))
     e = O.treecode(float(g["L"]), float(g["eps"]), float(g["mac"]), int(g["degree"]), int(g["max_source"]),
