@@ -265,10 +265,18 @@ def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
         roof.update({"bound": "fp64-pipe", "peak": None, "frac": None, "mufu_convention": None,
                      "peak_source": "FP64 pipe (reference arithmetic, bit-exact); not a speed-of-light kernel"})
     elif a.field.startswith("treecode"):
-        roof.update({"bound": "mufu", "peak": mufu_peak / 1e9, "unit": "Gpair/s (direct-equivalent)",
-                     "frac": None, "mufu_convention": None,
-                     "peak_source": "near-field pairs need one MUFU rsqrt each (16/clk/SM)",
-                     "note": "achieved is direct-equivalent N^2 pairs per near-kernel time; see kernel_evals_per_s"})
+        # actual near-field pairs (counted on the device while profiling) per
+        # near-kernel time, against one MUFU rsqrt per pair
+        import multi_species_b200 as M
+        near_pairs = M.profile_read("treecode_near_pairs")[2]
+        ach = near_pairs / (kms / 1e3) if kms > 0 else 0.0
+        roof.update({"bound": "mufu", "peak": mufu_peak / 1e9, "unit": "Gpair/s (near-field pairs)",
+                     "achieved": ach / 1e9, "frac": ach / mufu_peak if a.field == "treecode32c" else None,
+                     "mufu_convention": None, "pairs_per_launch": near_pairs / kl if kl else None,
+                     "traffic": None,
+                     "peak_source": f"{sm} SMs x {MUFU_PER_CLK_PER_SM} MUFU/clk x sm_max_mhz {mhz:.0f}: each "
+                                    "near-field band pair needs one MUFU rsqrt",
+                     "direct_equivalent_per_s": achieved / 1e9})
     return roof
 
 

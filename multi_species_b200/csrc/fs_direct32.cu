@@ -297,41 +297,44 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             // band tiles (every pair of the warp within |d| <= band, one image
             // per target): q/2 * d * y with y = rsqrt(d^2 + eps^2), two targets
             // per packed FP32x2 op, Kahan-compensated
-            const float2 e2b = make_float2(eps2, eps2);
-            float2 tau2[kR / 2], acc2[kR / 2], cmp2[kR / 2];
+            const float2 e2b = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
+            float2 tau2[kR / 2], acc2[kR / 2], ncmp2[kR / 2];
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
                 tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
                 acc2[h] = make_float2(0.f, 0.f);
-                cmp2[h] = make_float2(0.f, 0.f);
+                ncmp2[h] = make_float2(0.f, 0.f);
             }
 #pragma unroll 2
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
-                const float2 nsx = make_float2(-e.x, -e.x);
+                const float2 sx2 = make_float2(e.x, e.x);
                 const float2 qh = make_float2(e.y, e.y);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
-                    const float2 d = __fadd2_rn(tau2[h], nsx);
+                    // differences as FMAs with -1 (exact products), so no sign
+                    // flips are needed: d = tau - s, then Kahan with the
+                    // negated compensation nc = -c
+                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
                     const float2 r2 = __ffma2_rn(d, d, e2b);
                     const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
                     const float2 g = __fmul2_rn(d, y);
-                    const float2 v = __ffma2_rn(qh, g, make_float2(-cmp2[h].x, -cmp2[h].y));
+                    const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
                     const float2 sum = __fadd2_rn(acc2[h], v);
-                    const float2 t = __fadd2_rn(sum, make_float2(-acc2[h].x, -acc2[h].y));
-                    cmp2[h] = __fadd2_rn(t, make_float2(-v.x, -v.y));
+                    const float2 t = __ffma2_rn(acc2[h], m1, sum);
+                    ncmp2[h] = __ffma2_rn(t, m1, v);
                     acc2[h] = sum;
                 }
             }
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
-                acc64[2 * h] += (double)acc2[h].x - (double)cmp2[h].x;
-                acc64[2 * h + 1] += (double)acc2[h].y - (double)cmp2[h].y;
+                acc64[2 * h] += (double)acc2[h].x + (double)ncmp2[h].x;
+                acc64[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
             }
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
             // two targets per packed FP32x2 op, one MUFU.RCP per two targets
-            const float2 e2v = make_float2(Jb.e2f, Jb.e2f);
+            const float2 e2v = make_float2(Jb.e2f, Jb.e2f), m1 = make_float2(-1.f, -1.f);
             float2 tau2[kR / 2], acc2[kR / 2];
 #pragma unroll
             for (int h = 0; h < kR / 2; ++h) {
@@ -341,11 +344,11 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
 #pragma unroll 4
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
-                const float2 nsx = make_float2(-e.x, -e.x);
+                const float2 sx2 = make_float2(e.x, e.x);
                 const float2 qa1 = make_float2(e.z, e.z);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
-                    const float2 d = __fadd2_rn(tau2[h], nsx);
+                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
                     const float2 r2 = __ffma2_rn(d, d, e2v);
                     const float W = rcp_approx(r2.x * r2.y);
                     // (r_a W, r_b W) = (w'_b, w'_a): the lanes come out swapped,

@@ -67,6 +67,9 @@ struct ProfNode {
 void prof_capture_sink(std::vector<ProfNode>* sink);
 void prof_harvest(const std::vector<ProfNode>& nodes);  // events must have completed
 void prof_release(std::vector<ProfNode>& nodes);
+// Adds algorithmic work counted apart from any launch (e.g. the treecode's
+// near pairs and far terms) under `name` while profiling is enabled.
+void prof_add_work(const char* name, double work);
 
 // ------------------------------------------------------------------ device buffers
 // Bumped by every device (re)allocation of a DevBuf; a captured CUDA graph

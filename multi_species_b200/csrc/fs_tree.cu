@@ -614,7 +614,7 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
             const double sl = range_sum(pl, nd.m0, nd.m1 + 1), slx = range_sum(plx, nd.m0, nd.m1 + 1);
 #pragma unroll
             for (int r = 0; r < kNearR; ++r) exact[r] -= cbg * (xt[r] * sl - slx);
-            const float2 e2v = make_float2(eps2, eps2);
+            const float2 e2v = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
             for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile) {
                 const int cnt = min(kNearTile, nd.m1 - t0 + 1);
                 const double base = sx[t0];
@@ -622,35 +622,37 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
                 for (int k = threadIdx.x; k < cnt; k += kNearThreads)
                     shb[k] = make_float2((float)(sx[t0 + k] - base), (float)(0.5 * lam[t0 + k]));
                 __syncthreads();
-                float2 tau2[kNearR / 2], acc2[kNearR / 2], cmp2[kNearR / 2];
+                float2 tau2[kNearR / 2], acc2[kNearR / 2], ncmp2[kNearR / 2];
 #pragma unroll
                 for (int h = 0; h < kNearR / 2; ++h) {
                     tau2[h] = make_float2((float)(xt[2 * h] - base), (float)(xt[2 * h + 1] - base));
                     acc2[h] = make_float2(0.f, 0.f);
-                    cmp2[h] = make_float2(0.f, 0.f);
+                    ncmp2[h] = make_float2(0.f, 0.f);
                 }
 #pragma unroll 2
                 for (int k = 0; k < cnt; ++k) {
                     const float2 e = shb[k];
-                    const float2 nsx = make_float2(-e.x, -e.x);
+                    const float2 sx2 = make_float2(e.x, e.x);
                     const float2 qh = make_float2(e.y, e.y);
 #pragma unroll
                     for (int h = 0; h < kNearR / 2; ++h) {
-                        const float2 d = __fadd2_rn(tau2[h], nsx);
+                        // differences as FMAs with -1 (exact products): no sign
+                        // flips; Kahan with the negated compensation nc = -c
+                        const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
                         const float2 r2 = __ffma2_rn(d, d, e2v);
                         const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
                         const float2 g = __fmul2_rn(d, y);
-                        const float2 v = __ffma2_rn(qh, g, make_float2(-cmp2[h].x, -cmp2[h].y));
+                        const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
                         const float2 sum = __fadd2_rn(acc2[h], v);
-                        const float2 t = __fadd2_rn(sum, make_float2(-acc2[h].x, -acc2[h].y));
-                        cmp2[h] = __fadd2_rn(t, make_float2(-v.x, -v.y));
+                        const float2 t = __ffma2_rn(acc2[h], m1, sum);
+                        ncmp2[h] = __ffma2_rn(t, m1, v);
                         acc2[h] = sum;
                     }
                 }
 #pragma unroll
                 for (int h = 0; h < kNearR / 2; ++h) {
-                    fp[2 * h] += (double)acc2[h].x - (double)cmp2[h].x;
-                    fp[2 * h + 1] += (double)acc2[h].y - (double)cmp2[h].y;
+                    fp[2 * h] += (double)acc2[h].x + (double)ncmp2[h].x;
+                    fp[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
                 }
             }
         } else {
@@ -724,6 +726,8 @@ class Treecode final : public FieldEngine {
         double h[2] = {0, 0};
         FS_CUDA(cudaMemcpyAsync(h, work_.p, sizeof(h), cudaMemcpyDeviceToHost, st));
         FS_CUDA(cudaStreamSynchronize(st));
+        prof_add_work("treecode_near_pairs", h[0]);
+        prof_add_work("treecode_far_terms", h[1]);
         return h[0] + h[1];
     }
 

@@ -138,6 +138,12 @@ void prof_harvest(const std::vector<ProfNode>& nodes) {
     }
 }
 
+void prof_add_work(const char* name, double work) {
+    if (!profiling_enabled()) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_totals[name].work += work;
+}
+
 void prof_release(std::vector<ProfNode>& nodes) {
     for (auto& n : nodes) {
         cudaEventDestroy(n.a);
