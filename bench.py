@@ -228,11 +228,19 @@ def run_reference(a, rank, world):
     v = statistics.median(x["value"] for x in vals)
     cb = dict(vals[-1])
     cb["value"] = v
+    from multi_species_b200 import decks
+    n = decks.deck_points(deck)
     return {"metric": "pair-interactions/s", "value": v, "unit": "pair-interactions/s", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (deck-generated point set)",
             "impl": "reference",
-            "config": {"workload": name, "points": None, "field": "reference E_MQ_DirectSum (CPU, OpenMP)"},
+            # one RK4 step is four evaluations of n x n pairs; each timed step here
+            # is a bounded sample of one evaluation, so the step time is extrapolated
+            "ms_per_step": 4.0 * n * n / v * 1e3,
+            "config": {"workload": name, "points": n, "eps": deck["greens_epsilon"], "dt": deck["dt"],
+                       "remesh_period": deck["remesh_period"],
+                       "field": ("reference E_MQ_Treecode (CPU, serial as shipped)" if tree
+                                 else "reference E_MQ_DirectSum (CPU, OpenMP)")},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
