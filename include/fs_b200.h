@@ -264,6 +264,26 @@ fs_status fs_pool_stats(fs_pool* pool, fs_pool_stats_t* stats);
 /* Device bytes the pool reserves for a simulation of these parameters. */
 fs_status fs_pool_estimate_bytes(const fs_sim_params* params, double* bytes);
 
+/* ----------------------------------------------------- diagnostic output */
+/* Write the reference's diagnostic and restart files for this session
+ * (AMRStructure::write_to_file, AMRStructure_io.cpp:8-101 and
+ * AMRStructure_restart.cpp:33-98; evaluate_field_uniform_grid's reduced-grid
+ * dump, AMRSimulation_field.cpp:81-111) under <sim_dir>simulation_output/:
+ * <species>/{xs/xs_,ps/ps_,fs/fs_}<iter> (raw FP64),
+ * <species>/panels/leaf_point_inds_<iter> (int32 x 9 per leaf),
+ * <species>/panels/full_tree_<iter> (int64 count + 80-byte panel records),
+ * reduce_xs/xs_<iter> and reduced_es/es_<iter> (raw FP64).  Particle files are
+ * written now (the constructor's dump) and after every step whose iteration is a
+ * multiple of diag_phase_space_period; reduced-grid files at reduced
+ * evaluations (start, remesh) on multiples of diag_period.  Copies go to pinned
+ * host memory on the session's stream and a writer thread writes the files
+ * while the next steps run.  species_names (num_species entries, NULL = species0,
+ * species1, ...) name the directories.  Directories are created as needed. */
+fs_status fs_sim_set_output(fs_sim* sim, const char* sim_dir, const char* const* species_names, int diag_period,
+                            int diag_phase_space_period);
+/* Wait until every queued file is written; FS_ERR_STATE if a write failed. */
+fs_status fs_sim_flush_output(fs_sim* sim);
+
 /* ------------------------------------------------------------- host mesh */
 /* Sizes of the uniform periodic panel mesh of create_prerefined_mesh. */
 fs_status fs_mesh_sizes(int initial_height, int p_height, int* npoints, int* npanels, int* nleaves);

@@ -44,7 +44,8 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_batch_remove", "fs_batch_step", "fs_batch_export", "fs_batch_info", "fs_batch_step_times",
            "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
            "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
-           "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes"]
+           "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes", "fs_sim_set_output",
+           "fs_sim_flush_output"]
 
 
 class FsError(RuntimeError):
@@ -124,6 +125,10 @@ def lib():
         L.fs_sim_pair_count.argtypes = [C.c_void_p, _dp]
         L.fs_sim_step_times.argtypes = [C.c_void_p, _dp, C.c_int, _ip]
         L.fs_sim_work.argtypes = [C.c_void_p, _dp, _dp]
+        L.fs_sim_set_output.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int, C.c_int]
+        L.fs_sim_set_output.restype = st
+        L.fs_sim_flush_output.argtypes = [C.c_void_p]
+        L.fs_sim_flush_output.restype = st
         L.fs_profile_enable.argtypes = [C.c_int]
         L.fs_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), _dp, _dp]
         L.fs_profile_reset.argtypes = []
@@ -351,6 +356,22 @@ class Simulation:
             _check(lib().fs_sim_num_points(self._h, s, C.byref(n)))
             self.species_points.append(n.value)
         self.num_steps = int(deck.get("num_steps", 10))
+
+    def set_output(self, sim_dir: str, diag_period: int | None = None,
+                   diag_phase_space_period: int | None = None) -> None:
+        """Write the reference's diagnostic files (xs/ps/fs, leaf_point_inds,
+        full_tree, reduce_xs/reduced_es) under sim_dir/simulation_output/,
+        species directories named by the deck; periods default to the deck's
+        diag_period / diag_phase_space_period (AMRSimulation_load.cpp:38-39)."""
+        dp = int(diag_period if diag_period is not None else self.deck.get("diag_period", 1))
+        pp = int(diag_phase_space_period if diag_phase_space_period is not None
+                 else self.deck.get("diag_phase_space_period", 1))
+        names = [str(sp.get("name", f"species{i}")).encode() for i, sp in enumerate(self.deck["species_list"])]
+        arr = (C.c_char_p * len(names))(*names)
+        _check(lib().fs_sim_set_output(self._h, str(sim_dir).encode(), arr, dp, pp))
+
+    def flush_output(self) -> None:
+        _check(lib().fs_sim_flush_output(self._h))
 
     def step(self, n: int = 1) -> None:
         """n x AMRSimulation::step (AMRSimulation_step.cpp:5-99)."""

@@ -35,6 +35,8 @@
 #include <cmath>
 #include <condition_variable>
 #include <deque>
+#include <filesystem>
+#include <fstream>
 #include <mutex>
 #include <thread>
 #include <array>
@@ -519,6 +521,183 @@ struct SpeciesState {
     DevBuf<int> inv, col_off, col_idx;
 };
 
+// ------------------------------------------------------------------ diagnostic output
+// The reference's dump files (AMRStructure_io.cpp:8-101, AMRStructure_restart.cpp:33-98,
+// AMRSimulation_field.cpp:81-111), under <sim_dir>simulation_output/:
+//   <species>/xs/xs_<iter>, ps/ps_<iter>, fs/fs_<iter>    raw FP64, one per point
+//   <species>/panels/leaf_point_inds_<iter>                int32 x 9 per leaf, leaf order
+//   <species>/panels/full_tree_<iter>                      int64 count, then one
+//       80-byte record per panel: index, level, parent, which child, 9 point
+//       indices, left/top/right/bottom neighbours, first child (int32), then
+//       left/right boundary, refined in xp / in p, needs refinement (int8), 3 pad
+//   reduce_xs/xs_<iter>, reduced_es/es_<iter>              raw FP64, reduced grid
+// Particle files are written every diag_phase_space_period steps (and at
+// iteration 0), reduced-grid files at reduced evaluations (start, remesh) on
+// multiples of diag_period.  The state is copied to pinned host memory on the
+// simulation stream and a writer thread writes the files while the next steps
+// run; two buffer sets alternate.
+struct DiagOutput {
+    // one full_tree record: 18 int32 (72 bytes), 5 int8 flags, 3 pad bytes
+    static constexpr size_t kTreeRecord = 18 * sizeof(int32_t) + 8;
+    static_assert(kTreeRecord == 80, "panel record layout");
+    struct Species {
+        std::string name;
+        int start = 0, n = 0;
+        const HostMesh* mesh = nullptr;
+    };
+    struct Slot {
+        double* host = nullptr;
+        cudaEvent_t ev = nullptr;
+        bool busy = false, particles = false, reduced = false;
+        int iter = 0;
+    };
+    std::string out;  // <sim_dir>simulation_output/
+    std::vector<Species> sp;
+    int diag_period = 1, phase_period = 1, device = 0;
+    int N = 0, U = 0;
+    Slot slot[2];
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<int> queue;
+    bool stop = false;
+    std::string error;
+
+    ~DiagOutput() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        if (th.joinable()) th.join();
+        for (auto& s : slot) {
+            if (s.host) cudaFreeHost(s.host);
+            if (s.ev) cudaEventDestroy(s.ev);
+        }
+    }
+
+    void start() {
+        for (auto& s : slot) {
+            FS_CUDA(cudaHostAlloc((void**)&s.host, sizeof(double) * (3 * (size_t)N + 2 * (size_t)U), 0));
+            FS_CUDA(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+        }
+        th = std::thread([this] { writer(); });
+    }
+
+    // Copy the state (and the reduced grid) for iteration `iter` on `st`.
+    void enqueue(cudaStream_t st, int iter, bool particles, bool reduced, const double* x, const double* p,
+                 const double* f, const double* rx, const double* re) {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return !slot[0].busy || !slot[1].busy; });
+        if (!error.empty()) fail(FS_ERR_STATE, "diagnostic output failed: " + error);
+        const int k = slot[0].busy ? 1 : 0;
+        Slot& S = slot[k];
+        S.busy = true;
+        S.iter = iter;
+        S.particles = particles;
+        S.reduced = reduced;
+        lk.unlock();
+        const size_t n = sizeof(double) * (size_t)N, u = sizeof(double) * (size_t)U;
+        if (particles) {
+            FS_CUDA(cudaMemcpyAsync(S.host, x, n, cudaMemcpyDeviceToHost, st));
+            FS_CUDA(cudaMemcpyAsync(S.host + N, p, n, cudaMemcpyDeviceToHost, st));
+            FS_CUDA(cudaMemcpyAsync(S.host + 2 * (size_t)N, f, n, cudaMemcpyDeviceToHost, st));
+        }
+        if (reduced) {
+            FS_CUDA(cudaMemcpyAsync(S.host + 3 * (size_t)N, rx, u, cudaMemcpyDeviceToHost, st));
+            FS_CUDA(cudaMemcpyAsync(S.host + 3 * (size_t)N + U, re, u, cudaMemcpyDeviceToHost, st));
+        }
+        FS_CUDA(cudaEventRecord(S.ev, st));
+        lk.lock();
+        queue.push_back(k);
+        cv.notify_all();
+    }
+
+    void flush() {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return queue.empty() && !slot[0].busy && !slot[1].busy; });
+        if (!error.empty()) {
+            const std::string e = error;
+            error.clear();
+            fail(FS_ERR_STATE, "diagnostic output failed: " + e);
+        }
+    }
+
+    static void write_file(const std::string& path, const void* data, size_t bytes) {
+        std::filesystem::create_directories(std::filesystem::path(path).parent_path());
+        std::ofstream o(path, std::ios::out | std::ios::binary);
+        if (!o) throw std::runtime_error("unable to open " + path);
+        o.write(static_cast<const char*>(data), (std::streamsize)bytes);
+        if (!o.good()) throw std::runtime_error("error writing " + path);
+    }
+
+    void write_slot(const Slot& S) {
+        const std::string it = std::to_string(S.iter);
+        if (S.particles) {
+            for (const auto& q : sp) {
+                const std::string d = out + q.name + "/";
+                write_file(d + "xs/xs_" + it, S.host + q.start, sizeof(double) * q.n);
+                write_file(d + "ps/ps_" + it, S.host + N + q.start, sizeof(double) * q.n);
+                write_file(d + "fs/fs_" + it, S.host + 2 * (size_t)N + q.start, sizeof(double) * q.n);
+                const HostMesh& M = *q.mesh;
+                std::vector<int32_t> inds;
+                inds.reserve(M.leaves.size() * 9);
+                for (int l : M.leaves)
+                    for (int k = 0; k < 9; ++k) inds.push_back(M.panels[l].pts[k]);
+                write_file(d + "panels/leaf_point_inds_" + it, inds.data(), sizeof(int32_t) * inds.size());
+                std::vector<unsigned char> tree(8 + kTreeRecord * M.panels.size(), 0);
+                const int64_t np = (int64_t)M.panels.size();
+                std::memcpy(tree.data(), &np, 8);
+                for (size_t i = 0; i < M.panels.size(); ++i) {
+                    const HostPanel& P = M.panels[i];
+                    const int32_t v[18] = {(int32_t)i, P.level, P.parent, P.which, P.pts[0], P.pts[1], P.pts[2],
+                                           P.pts[3], P.pts[4], P.pts[5], P.pts[6], P.pts[7], P.pts[8], P.left,
+                                           P.top, P.right, P.bottom, P.child};
+                    unsigned char* r = tree.data() + 8 + kTreeRecord * i;
+                    std::memcpy(r, v, sizeof(v));
+                    const int8_t b[5] = {(int8_t)(P.lb ? 1 : 0), (int8_t)(P.rb ? 1 : 0), (int8_t)(P.xp ? 1 : 0),
+                                         (int8_t)(P.pr ? 1 : 0), (int8_t)(P.needs ? 1 : 0)};
+                    std::memcpy(r + sizeof(v), b, 5);
+                }
+                write_file(d + "panels/full_tree_" + it, tree.data(), tree.size());
+            }
+        }
+        if (S.reduced) {
+            write_file(out + "reduce_xs/xs_" + it, S.host + 3 * (size_t)N, sizeof(double) * U);
+            write_file(out + "reduced_es/es_" + it, S.host + 3 * (size_t)N + U, sizeof(double) * U);
+        }
+    }
+
+    void writer() {
+        cudaSetDevice(device);
+        for (;;) {
+            int k;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return stop || !queue.empty(); });
+                if (queue.empty()) return;
+                k = queue.front();
+                queue.pop_front();
+            }
+            std::string err;
+            if (cudaEventSynchronize(slot[k].ev) != cudaSuccess) {
+                (void)cudaGetLastError();
+                err = "copy to host failed";
+            } else {
+                try {
+                    write_slot(slot[k]);
+                } catch (const std::exception& e) {
+                    err = e.what();
+                }
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            if (!err.empty() && error.empty()) error = err;
+            slot[k].busy = false;
+            cv.notify_all();
+        }
+    }
+};
+
 // Drive-field amplitude at time t (src/FieldStructure.cpp:15-96): ExternalTanh
 // (type 0, its factor k included) switches on around t = 69 and off around
 // t = 307 with widths 20, normalised to start from zero at t = 0; ExternalSine
@@ -555,8 +734,11 @@ struct Sim {
     Stage base;
 
     bool own_stream = true;
+    std::unique_ptr<DiagOutput> out;
+    int last_reduced_iter = 0;  // iteration of the last reduced-grid evaluation
 
     ~Sim() {
+        out.reset();  // writes what is queued
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (st && own_stream) cudaStreamDestroy(st);
@@ -800,6 +982,7 @@ struct Sim {
         FS_LAUNCHED((long long)sp.size());
     }
     void reduced_field() {
+        last_reduced_iter = iter;
         reduced_pre();
         run_call(reduced_call());
         reduced_post();
@@ -873,6 +1056,7 @@ struct Sim {
             t += prm.dt;
             remeshing = (iter % prm.remesh_period == 0);
             if (remeshing) {
+                last_reduced_iter = iter;
                 remesh_kernels();
                 reduced_pre();
             }
@@ -906,6 +1090,42 @@ struct Sim {
             run_call(call(c));
             post_call(c);
         }
+        dump(remeshing);
+    }
+
+    // AMRSimulation::step writes the particles every diag_phase_space_period
+    // steps (AMRSimulation_step.cpp:94-96); evaluate_field_uniform_grid writes the
+    // reduced grid on multiples of diag_period (AMRSimulation_field.cpp:81).
+    void dump(bool reduced_now) {
+        if (!out) return;
+        const bool particles = iter % out->phase_period == 0;
+        const bool reduced = reduced_now && iter % out->diag_period == 0;
+        if (particles || reduced) out->enqueue(st, iter, particles, reduced, x.p, p.p, f.p, rx.p, re.p);
+    }
+
+    void set_output(const std::string& sim_dir, const std::vector<std::string>& names, int diag_period,
+                    int phase_period) {
+        if (diag_period < 1 || phase_period < 1) fail(FS_ERR_ARG, "diagnostic periods must be >= 1");
+        out.reset();
+        auto o = std::make_unique<DiagOutput>();
+        o->out = sim_dir + ((sim_dir.empty() || sim_dir.back() == '/') ? "" : "/") + "simulation_output/";
+        o->diag_period = diag_period;
+        o->phase_period = phase_period;
+        o->device = prm.device;
+        o->N = N;
+        o->U = U;
+        for (size_t k = 0; k < sp.size(); ++k) {
+            DiagOutput::Species q;
+            q.name = k < names.size() && !names[k].empty() ? names[k] : "species" + std::to_string(k);
+            q.start = sp[k]->start;
+            q.n = sp[k]->n;
+            q.mesh = &sp[k]->mesh;
+            o->sp.push_back(q);
+        }
+        o->start();
+        out = std::move(o);
+        // the state as it stands (the ctor's dump at iteration 0)
+        dump(last_reduced_iter == iter);
     }
 
     static int* field_error_flag(FieldEngine* fe) { return fe->error_flag(); }
@@ -965,7 +1185,30 @@ fs_status fs_sim_remesh(fs_sim* sim) {
         if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
         FS_CUDA(cudaSetDevice(sim->impl.prm.device));
         sim->impl.remesh();
+        if (sim->impl.out && sim->impl.iter % sim->impl.out->diag_period == 0)
+            sim->impl.out->enqueue(sim->impl.st, sim->impl.iter, false, true, nullptr, nullptr, nullptr,
+                                   sim->impl.rx.p, sim->impl.re.p);
         sim->impl.check_status();
+    });
+}
+
+fs_status fs_sim_set_output(fs_sim* sim, const char* sim_dir, const char* const* species_names, int diag_period,
+                            int diag_phase_space_period) {
+    return fsb::guard([&] {
+        if (!sim || !sim_dir) fsb::fail(FS_ERR_ARG, "null argument");
+        auto& S = sim->impl;
+        FS_CUDA(cudaSetDevice(S.prm.device));
+        std::vector<std::string> names;
+        for (int k = 0; k < S.prm.num_species; ++k)
+            names.push_back(species_names && species_names[k] ? species_names[k] : "");
+        S.set_output(sim_dir, names, diag_period, diag_phase_space_period);
+    });
+}
+
+fs_status fs_sim_flush_output(fs_sim* sim) {
+    return fsb::guard([&] {
+        if (!sim) fsb::fail(FS_ERR_ARG, "null sim");
+        if (sim->impl.out) sim->impl.out->flush();
     });
 }
 
