@@ -43,11 +43,11 @@ sys.path.insert(0, ROOT)
 
 MUFU_PER_CLK_PER_SM = 16          # MUFU (rsqrt / rcp) lanes per clock per SM
 FP32_LANES_PER_CLK_PER_SM = 128    # FP32 FMA-pipe lanes per clock per SM
-# FP32 lane-operations per far pair in k_pairs32 (FADD2, FFMA2, FMUL2, FFMA2
-# over two targets = 8, plus one FMUL for the shared reciprocal = 9 per two
-# pairs); its MUFU use is 0.5 per pair (32 pairs/clk/SM), so the FP32 datapath
-# (128 / 4.5 = 28.4 pairs/clk/SM) is the bound.
-PAIR32_FP32_OPS = 4.5
+# FP32 lane-operations per far pair in k_pairs32 (FFMA2 difference, FFMA2
+# square, FFMA2 accumulate over two targets = 6, plus the scalar FMULs for
+# r_a r_b and q W = 8 per two pairs); its MUFU use is 0.5 per pair, so the FP32
+# datapath (128 / 4 = 32 pairs/clk/SM) and MUFU (16 x 2 = 32) bound it alike.
+PAIR32_FP32_OPS = 4.0
 
 
 def parse():

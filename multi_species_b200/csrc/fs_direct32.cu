@@ -207,8 +207,8 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // series v/2 + v^2/8 + v^3/32 + ... matches c = v/2 + v^2/8 + v^3/16 + ... to
 // second order: the error is below v^2/16 <= 1e-6 of c at the band edge
 // (2e-9 of the pair's q/2) and falls off as 1/d^6.  Far pairs need no square
-// root and one FMA for the series, and two targets share one MUFU.RCP:
-// w'_a = r_b / (r_a r_b).
+// root, and two targets share one MUFU.RCP and one scalar product:
+// q a1 / r_a = (q a1 / (r_a r_b)) r_b.
 #ifndef FS_PAIR_BAND
 #define FS_PAIR_BAND 16.0
 #endif
@@ -345,16 +345,16 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
                 const float2 sx2 = make_float2(e.x, e.x);
-                const float2 qa1 = make_float2(e.z, e.z);
 #pragma unroll
                 for (int h = 0; h < kR / 2; ++h) {
                     const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
                     const float2 r2 = __ffma2_rn(d, d, e2v);
-                    const float W = rcp_approx(r2.x * r2.y);
-                    // (r_a W, r_b W) = (w'_b, w'_a): the lanes come out swapped,
-                    // so acc2[h].x accumulates target 2h+1 and .y target 2h
-                    const float2 w = __fmul2_rn(r2, make_float2(W, W));
-                    acc2[h] = __ffma2_rn(w, qa1, acc2[h]);
+                    // q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b): one
+                    // reciprocal and one scalar product serve both targets, and
+                    // (qW r_a, qW r_b) are the terms of targets 2h+1 and 2h, so
+                    // acc2[h].x accumulates target 2h+1 and .y target 2h
+                    const float qW = e.z * rcp_approx(r2.x * r2.y);
+                    acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
                 }
             }
 #pragma unroll
