@@ -581,7 +581,7 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
          const double* __restrict__ efar, const int* __restrict__ sidx, double L, double eps, double cbg, double norm,
          Stage S, int* __restrict__ err) {
     __shared__ float4 shg[kNearTile];          // general path: {s, lambda/2, lambda/2 a1, lambda/2 a2}
-    __shared__ float2 shb[kNearTile];          // band path: {s, lambda/2}
+    __shared__ __align__(16) float2 shb[2][kNearTile];  // band path: {s, lambda/2}, double-buffered
     const int l = blockIdx.x;
     if (l >= meta[1] || meta[2]) return;
     const TNode leaf = nodes[leaves[l]];
@@ -615,13 +615,34 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
 #pragma unroll
             for (int r = 0; r < kNearR; ++r) exact[r] -= cbg * (xt[r] * sl - slx);
             const float2 e2v = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
-            for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile) {
+            // software pipeline: each thread holds two sources of the next tile
+            // in registers while the current tile is computed; one barrier per tile
+            constexpr int kPer = kNearTile / kNearThreads;
+            double nx[kPer], nl[kPer];
+            double nbase = sx[nd.m0];
+            auto fetch = [&](int t0) {
+#pragma unroll
+                for (int i = 0; i < kPer; ++i) {
+                    const int j = t0 + threadIdx.x + i * kNearThreads;
+                    nx[i] = (j <= nd.m1) ? sx[j] : 0.0;
+                    nl[i] = (j <= nd.m1) ? lam[j] : 0.0;
+                }
+                nbase = sx[t0];
+            };
+            fetch(nd.m0);
+            int buf = 0;
+            for (int t0 = nd.m0; t0 <= nd.m1; t0 += kNearTile, buf ^= 1) {
                 const int cnt = min(kNearTile, nd.m1 - t0 + 1);
-                const double base = sx[t0];
+                const double base = nbase;
+#pragma unroll
+                for (int i = 0; i < kPer; ++i) {
+                    const int k = threadIdx.x + i * kNearThreads;
+                    // padding sources (q = 0, s = 0) complete the last pair
+                    shb[buf][k] = (k < cnt) ? make_float2((float)(nx[i] - base), (float)(0.5 * nl[i]))
+                                            : make_float2(0.f, 0.f);
+                }
                 __syncthreads();
-                for (int k = threadIdx.x; k < cnt; k += kNearThreads)
-                    shb[k] = make_float2((float)(sx[t0 + k] - base), (float)(0.5 * lam[t0 + k]));
-                __syncthreads();
+                if (t0 + kNearTile <= nd.m1) fetch(t0 + kNearTile);
                 float2 tau2[kNearR / 2], acc2[kNearR / 2], ncmp2[kNearR / 2];
 #pragma unroll
                 for (int h = 0; h < kNearR / 2; ++h) {
@@ -629,24 +650,29 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
                     acc2[h] = make_float2(0.f, 0.f);
                     ncmp2[h] = make_float2(0.f, 0.f);
                 }
+                const float4* pairs = reinterpret_cast<const float4*>(shb[buf]);
+                const int npair = (cnt + 1) >> 1;
 #pragma unroll 2
-                for (int k = 0; k < cnt; ++k) {
-                    const float2 e = shb[k];
-                    const float2 sx2 = make_float2(e.x, e.x);
-                    const float2 qh = make_float2(e.y, e.y);
+                for (int k = 0; k < npair; ++k) {
+                    const float4 e4 = pairs[k];  // two sources per shared-memory load
 #pragma unroll
-                    for (int h = 0; h < kNearR / 2; ++h) {
-                        // differences as FMAs with -1 (exact products): no sign
-                        // flips; Kahan with the negated compensation nc = -c
-                        const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
-                        const float2 r2 = __ffma2_rn(d, d, e2v);
-                        const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                        const float2 g = __fmul2_rn(d, y);
-                        const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
-                        const float2 sum = __fadd2_rn(acc2[h], v);
-                        const float2 t = __ffma2_rn(acc2[h], m1, sum);
-                        ncmp2[h] = __ffma2_rn(t, m1, v);
-                        acc2[h] = sum;
+                    for (int u = 0; u < 2; ++u) {
+                        const float2 sx2 = u ? make_float2(e4.z, e4.z) : make_float2(e4.x, e4.x);
+                        const float2 qh = u ? make_float2(e4.w, e4.w) : make_float2(e4.y, e4.y);
+#pragma unroll
+                        for (int h = 0; h < kNearR / 2; ++h) {
+                            // differences as FMAs with -1 (exact products): no sign
+                            // flips; Kahan with the negated compensation nc = -c
+                            const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
+                            const float2 r2 = __ffma2_rn(d, d, e2v);
+                            const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                            const float2 g = __fmul2_rn(d, y);
+                            const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
+                            const float2 sum = __fadd2_rn(acc2[h], v);
+                            const float2 t = __ffma2_rn(acc2[h], m1, sum);
+                            ncmp2[h] = __ffma2_rn(t, m1, v);
+                            acc2[h] = sum;
+                        }
                     }
                 }
 #pragma unroll
@@ -655,6 +681,7 @@ k_near32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const in
                     fp[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
                 }
             }
+            __syncthreads();  // the general path and the next leaf reuse shared memory
         } else {
 #pragma unroll 1
             for (int r = 0; r < kNearR; ++r)
