@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
     const double* cheb = consts;
     const double* wk = consts + (kMaxDegree + 1);
     const int PP = P + 1;
-    __shared__ double red[256];
+    __shared__ double red[8 * (kMaxDegree + 1)];  // per warp (256 threads), per moment
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
         // node owning this item: last node with item_start <= item (nodes 1..nnodes-1)
         int lo = 1, hi = nnodes - 1;
@@ -312,7 +312,36 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
             double ak[kMaxDegree + 1];
             int exact = -1;
             double sum = 0.0;
-            for (int k = 0; k < PP; ++k) {
+            // w_k / dx_k, two nodes per division where both differences are
+            // clear of zero: 1/dx_a = dx_b / (dx_a dx_b) (a few ulps; |dx| lies
+            // between the spacing of doubles near x and the node width, so the
+            // product neither underflows nor overflows)
+            int k = 0;
+            for (; k + 1 < PP; k += 2) {
+                const double da = dsub(x, t[k]), db = dsub(x, t[k + 1]);
+                if (fabs(da) <= DBL_MIN || fabs(db) <= DBL_MIN) {
+                    if (fabs(da) <= DBL_MIN) {
+                        exact = k;
+                        ak[k] = 0.0;
+                    } else {
+                        ak[k] = ddiv(wk[k], da);
+                        sum = dadd(sum, ak[k]);
+                    }
+                    if (fabs(db) <= DBL_MIN) {
+                        exact = k + 1;
+                        ak[k + 1] = 0.0;
+                    } else {
+                        ak[k + 1] = ddiv(wk[k + 1], db);
+                        sum = dadd(sum, ak[k + 1]);
+                    }
+                } else {
+                    const double r = ddiv(1.0, dmul(da, db));
+                    ak[k] = dmul(wk[k], dmul(db, r));
+                    ak[k + 1] = dmul(wk[k + 1], dmul(da, r));
+                    sum = dadd(dadd(sum, ak[k]), ak[k + 1]);
+                }
+            }
+            if (k < PP) {
                 const double dx = dsub(x, t[k]);
                 if (fabs(dx) <= DBL_MIN) {
                     exact = k;
@@ -331,18 +360,23 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
             const double l = lam[j];
             for (int k = 0; k < PP; ++k) acc[k] = dadd(acc[k], dmul(dmul(ak[k], D), l));
         }
-        // block reduction of PP values, fixed order
+        // block reduction of PP values in a fixed order: a shuffle tree within
+        // each warp, then the eight warp sums in warp order
         double* out = partial + (size_t)item * (kMaxDegree + 1);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         for (int k = 0; k < PP; ++k) {
-            red[threadIdx.x] = acc[k];
-            __syncthreads();
-            for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
-                if (threadIdx.x < s) red[threadIdx.x] = dadd(red[threadIdx.x], red[threadIdx.x + s]);
-                __syncthreads();
-            }
-            if (threadIdx.x == 0) out[k] = red[0];
-            __syncthreads();
+            double v = acc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = dadd(v, __shfl_down_sync(0xffffffffu, v, o));
+            if (lane == 0) red[warp * (kMaxDegree + 1) + k] = v;
         }
+        __syncthreads();
+        if (threadIdx.x < PP) {
+            double sum = red[threadIdx.x];
+            for (int w = 1; w < 8; ++w) sum = dadd(sum, red[w * (kMaxDegree + 1) + threadIdx.x]);
+            out[threadIdx.x] = sum;
+        }
+        __syncthreads();
     }
 }
 
