@@ -105,6 +105,15 @@ typedef struct fs_species_params {
     double pmin, pmax;
     int ics_type;                 /* 1,2 Landau; 3 strong two-stream; 4 colder two-stream; 9,10 ion acoustic */
     double pth, pstr, amp, normalized_wavenumber;
+    /* Adaptive refinement (AMRSimulation_load.cpp:246-258; generate_mesh,
+     * AMRStructure_amr.cpp:901-941): when on, panels of the uniform mesh whose
+     * nine f values meet a criterion of amr_eps (spread, relative spread,
+     * max/min, x and p difference quotients, in that order) are split 2x2 up to
+     * max_height, at the start and at every remesh. */
+    int do_adaptively_refine;
+    int max_height;
+    int n_amr_eps;                /* 0..5; 0 turns the refinement off           */
+    double amr_eps[5];
 } fs_species_params;
 
 /* Deck-level parameters (AMRSimulation_load.cpp:14-47). */

@@ -62,7 +62,9 @@ class FieldParams(C.Structure):
 class SpeciesParams(C.Structure):
     _fields_ = [("q", C.c_double), ("m", C.c_double), ("initial_height", C.c_int), ("p_height", C.c_int),
                 ("pmin", C.c_double), ("pmax", C.c_double), ("ics_type", C.c_int), ("pth", C.c_double),
-                ("pstr", C.c_double), ("amp", C.c_double), ("normalized_wavenumber", C.c_double)]
+                ("pstr", C.c_double), ("amp", C.c_double), ("normalized_wavenumber", C.c_double),
+                ("do_adaptively_refine", C.c_int), ("max_height", C.c_int), ("n_amr_eps", C.c_int),
+                ("amr_eps", C.c_double * 5)]
 
 
 class SimParams(C.Structure):
@@ -329,6 +331,15 @@ def sim_params(deck: dict, field_backend: str | None = None, device: int = 0) ->
         S.ics_type = int(sp.get("ics_type", 1))
         S.pth, S.pstr, S.amp = float(sp.get("pth", 1.0)), float(sp.get("pstr", 0.0)), float(sp.get("amp", 0.0))
         S.normalized_wavenumber = float(sp.get("normalized_wavenumber", 1.0))
+        # adaptive refinement: off unless do_adaptively_refine and amr_epsilons
+        # are given (AMRSimulation_load.cpp:246-258)
+        eps = sp.get("amr_epsilons")
+        S.do_adaptively_refine = 1 if (bool(sp.get("do_adaptively_refine", False)) and eps is not None) else 0
+        S.max_height = int(sp.get("max_height", sp.get("initial_height", 6)))
+        eps = [float(e) for e in (eps or [])][:5]
+        S.n_amr_eps = len(eps)
+        for k, e in enumerate(eps):
+            S.amr_eps[k] = e
     P.device = int(device)
     # "external_field" block (AMRSimulation_load.cpp:98-136); absent = off
     ext = deck.get("external_field") or {}
@@ -411,6 +422,13 @@ class Simulation:
         return v.value
 
     def state(self) -> dict:
+        n = C.c_int()
+        _check(lib().fs_sim_num_points(self._h, -1, C.byref(n)))  # adaptive meshes change it at remesh
+        self.n = n.value
+        self.species_points = []
+        for s in range(self._p.num_species):
+            _check(lib().fs_sim_num_points(self._h, s, C.byref(n)))
+            self.species_points.append(n.value)
         a = {k: np.zeros(self.n) for k in ("xs", "ps", "fs", "q_ws", "es")}
         _check(lib().fs_sim_export(self._h, *(_ptr(a[k]) for k in ("xs", "ps", "fs", "q_ws", "es"))))
         return a

@@ -148,7 +148,13 @@ struct HostMesh {
     std::vector<HostPanel> panels;
     std::vector<double> xs, ps;
     std::vector<int> leaves;
+    int min_unrefined = 1;  // first panel of the last uniform generation
     void build(int h, int ph, double xmin, double xmax, double pmin, double pmax);
+    // Adaptive refinement (generate_mesh, AMRStructure_amr.cpp:901-941): f holds
+    // the values at the current points and grows with the mesh; eval(x, p, n, out)
+    // gives f at new points.
+    void adapt(std::vector<double>& f, const double* eps, int neps, int max_height,
+               const std::function<void(const double*, const double*, int, double*)>& eval);
     std::vector<double> base_weights(double q, int quadrature) const;
     void panel_records(int* out) const;  // 18 ints per panel
     int nx() const { return 2 * (1 << h) + 1; }

@@ -12,6 +12,7 @@
 // The mesh is identical at every remesh of a uniform deck, so it is built once
 // per species and cached on the device.
 #include <cmath>
+#include <functional>
 
 #include "fs_internal.h"
 
@@ -102,7 +103,10 @@ class Refiner {
                     link[S.own0][li] = link[S.own1][li] = -2;
                 } else if (nb == -1) {
                     HostPanel& pn = m_.panels[m_.panels[P.parent].*(S.nbr)];
-                    if (!pn.xp) pn.needs = 1;
+                    if (!pn.xp) {
+                        pn.needs = 1;
+                        need_further = true;
+                    }
                 } else if (m_.panels[nb].xp) {
                     const int c0 = m_.panels[nb].child + S.face0, c1 = m_.panels[nb].child + S.face1;
                     link[S.own0][li] = c0;
@@ -258,10 +262,14 @@ class Refiner {
         }
     }
 
+    // a coarser neighbour was flagged while splitting (2:1 balance)
+    bool need_further = false;
+
     void flag_generation() {
         for (size_t i = m_min_; i < m_.panels.size(); ++i) m_.panels[i].needs = 1;
     }
     void next_generation(int first) { m_min_ = first; }
+    int first() const { return m_min_; }
 
    private:
     HostMesh& m_;
@@ -347,6 +355,75 @@ void HostMesh::build(int h_, int ph_, double xmin_, double xmax_, double pmin_, 
     }
     collect_leaves(*this, 0, leaves);
     if (xs.size() != npts) fail(FS_ERR_STATE, "mesh point count mismatch");
+    min_unrefined = R.first();
+}
+
+namespace {
+
+// test_panel (AMRStructure_amr.cpp:971-1081): flags a panel below max_height
+// whose nine values meet a criterion: spread of f (eps0), spread relative to
+// the centre value (eps1), max/min ratio (eps2), largest x difference quotient
+// (eps3), p difference quotient (eps4: the reference reads six entries of
+// which it sets two, the rest uninitialised; the two it sets are used).
+bool test_panel(HostMesh& m, int pi, const std::vector<double>& f, const double* eps, int neps, int max_height) {
+    HostPanel& P = m.panels[pi];
+    double pf[9];
+    for (int i = 0; i < 9; ++i) pf[i] = f[P.pts[i]];
+    bool crit = false;
+    if (neps > 0) {
+        double mx = pf[0], mn = pf[0];
+        for (int i = 1; i < 9; ++i) {
+            if (mx < pf[i]) mx = pf[i];
+            if (mn > pf[i]) mn = pf[i];
+        }
+        crit = crit || (mx - mn > eps[0]);
+        if (neps > 1) crit = crit || (mx - mn) / pf[4] > eps[1];
+        if (neps > 2) crit = crit || mx / mn > eps[2];
+    }
+    if (neps > 3) {
+        const double dx = m.xs[P.pts[3]] - m.xs[P.pts[0]];
+        double md = std::fabs((pf[3] - pf[0]) / dx);
+        for (int i = 1; i < 6; ++i) {
+            const double v = std::fabs((pf[3 + i] - pf[i]) / dx);
+            if (md < v) md = v;
+        }
+        crit = crit || (md > eps[3]);
+    }
+    if (neps > 4) {
+        const double dp = m.ps[P.pts[1]] - m.ps[P.pts[0]];
+        double a[2] = {0.0, 0.0};
+        for (int jj = 0; jj < 3; ++jj)
+            for (int ii = 0; ii < 2; ++ii) a[ii] = std::fabs((pf[3 * jj + ii + 1] - pf[3 * jj + ii]) / dp);
+        crit = crit || ((a[0] < a[1] ? a[1] : a[0]) > eps[4]);
+    }
+    if (P.level < max_height && crit) {
+        P.needs = 1;
+        return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+void HostMesh::adapt(std::vector<double>& f, const double* eps, int neps, int max_height,
+                     const std::function<void(const double*, const double*, int, double*)>& eval) {
+    Refiner R(*this);
+    R.next_generation(min_unrefined);
+    bool need = false;
+    for (int i = min_unrefined; i < (int)panels.size(); ++i) need = test_panel(*this, i, f, eps, neps, max_height) || need;
+    while (need) {
+        need = false;
+        R.need_further = false;
+        const size_t n0 = xs.size();
+        R.split_xp();
+        need = R.need_further;
+        f.resize(xs.size());
+        if (xs.size() > n0) eval(xs.data() + n0, ps.data() + n0, (int)(xs.size() - n0), f.data() + n0);
+        for (int i = min_unrefined; i < (int)panels.size(); ++i)
+            if (!panels[i].xp) need = test_panel(*this, i, f, eps, neps, max_height) || need;
+    }
+    leaves.clear();
+    collect_leaves(*this, 0, leaves);
 }
 
 // set_leaves_weights without the final *f (AMRStructure_amr.cpp:1084-1151):

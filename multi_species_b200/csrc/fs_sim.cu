@@ -468,6 +468,59 @@ __global__ void k_eval_points(MeshView M, const double* __restrict__ sortx, cons
     fnew[order[k]] = v;
 }
 
+// interpolate_from_mesh (AMRStructure_interp.cpp:1094-1143) for the points an
+// adaptive refinement adds: shift_xs, the recursive search from the root of
+// the previous mesh, then its leaf's fit in the single-point expression
+// (:1086-1088) with one rounding per operation.
+__global__ void k_interp_points(MeshView M, const double* __restrict__ ox, const double* __restrict__ op, int n,
+                                const double* __restrict__ px, const double* __restrict__ pp,
+                                double* __restrict__ fout, int* __restrict__ status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double tp = pp[k];
+    double tx = px[k];
+    const double x_bl = ox[0], p_bl = op[0], x_tl = ox[2], p_tl = op[2];
+    const double x_br = ox[6], p_br = op[6], x_tr = ox[8], p_tr = op[8];
+    int cnt = 0;
+    while (!edge_left(x_tl, p_tl, x_bl, p_bl, tx, tp)) {
+        tx = dadd(tx, M.Lx);
+        if (++cnt > 10) {
+            raise_status(status, FS_ERR_SHIFT);
+            fout[k] = 0.0;
+            return;
+        }
+    }
+    cnt = 0;
+    while (!edge_right(x_tr, p_tr, x_br, p_br, tx, tp)) {
+        tx = dsub(tx, M.Lx);
+        if (++cnt > 10) {
+            raise_status(status, FS_ERR_SHIFT);
+            fout[k] = 0.0;
+            return;
+        }
+    }
+    bool beyond = false;
+    const int leaf = find_from_root(M, ox, op, tx, tp, beyond);
+    const int slot = (!beyond && leaf > 0) ? M.leaf_slot[leaf] : -1;
+    if (slot < 0) {
+        if (leaf < 0) raise_status(status, FS_ERR_WALK);
+        fout[k] = M.f_beyond;
+        return;
+    }
+    const double* c = M.coef + (size_t)slot * 11;
+    const double dx = dsub(tx, c[9]), dp = dsub(tp, c[10]);
+    double v = c[0];
+    v = dadd(v, dmul(c[1], dx));
+    v = dadd(v, dmul(dmul(c[2], dx), dp));
+    v = dadd(v, dmul(c[3], dp));
+    v = dadd(v, dmul(dmul(c[4], dx), dx));
+    v = dadd(v, dmul(dmul(dmul(c[5], dx), dx), dp));
+    v = dadd(v, dmul(dmul(dmul(dmul(c[6], dx), dx), dp), dp));
+    v = dadd(v, dmul(dmul(dmul(c[7], dx), dp), dp));
+    v = dadd(v, dmul(dmul(c[8], dp), dp));
+    fout[k] = v;
+}
+
 __global__ void k_reset_points(int n, const double* __restrict__ lat_x, const double* __restrict__ lat_p,
                                const double* __restrict__ w0, const double* __restrict__ fnew, double* __restrict__ x,
                                double* __restrict__ p, double* __restrict__ f, double* __restrict__ qw) {
@@ -496,10 +549,20 @@ __global__ void k_scatter_reduced(int n, const int* __restrict__ inv, const doub
     e[k] = re[inv[k]];
 }
 
+// Host-to-device copy that has landed when it returns.  cudaMemcpy from pageable
+// memory may return once the data is staged, with the DMA still queued on the
+// legacy default stream, which the library's non-blocking streams do not wait
+// for; the legacy stream is synchronised before any kernel can read the data.
+inline void h2d(void* dst, const void* src, size_t bytes) {
+    if (!bytes) return;
+    FS_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    FS_CUDA(cudaStreamSynchronize(nullptr));
+}
+
 template <class T>
 void upload(DevBuf<T>& b, const std::vector<T>& h) {
     b.ensure(h.size());
-    if (!h.empty()) FS_CUDA(cudaMemcpy(b.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    h2d(b.p, h.data(), sizeof(T) * h.size());
 }
 
 inline int blocks(int n, int per = kT) { return (n + per - 1) / per; }
@@ -507,7 +570,12 @@ inline int blocks(int n, int per = kT) { return (n + per - 1) / per; }
 }  // namespace
 
 struct SpeciesState {
-    HostMesh mesh;
+    HostMesh mesh;       // current mesh (uniform, or refined adaptively)
+    HostMesh base_mesh;  // the uniform mesh (adaptive species)
+    bool adaptive = false;
+    int max_height = 0, neps = 0;
+    double eps[5] = {0, 0, 0, 0, 0};
+    int nbase = 0;       // lattice points: the first nbase points of the species
     int start = 0, n = 0;
     double q = 0, m = 0, qm = 0, f_beyond = 0;
     int nleaves = 0, npx = 0, npp = 0;
@@ -540,21 +608,25 @@ struct DiagOutput {
     // one full_tree record: 18 int32 (72 bytes), 5 int8 flags, 3 pad bytes
     static constexpr size_t kTreeRecord = 18 * sizeof(int32_t) + 8;
     static_assert(kTreeRecord == 80, "panel record layout");
+    // What one dump writes for a species: its place in the state arrays and
+    // the files of its mesh as it stood when the dump was queued.
     struct Species {
         std::string name;
         int start = 0, n = 0;
-        const HostMesh* mesh = nullptr;
+        std::vector<int32_t> leaf_inds;
+        std::vector<unsigned char> tree;
     };
     struct Slot {
         double* host = nullptr;
+        size_t cap = 0;  // doubles
         cudaEvent_t ev = nullptr;
         bool busy = false, particles = false, reduced = false;
-        int iter = 0;
+        int iter = 0, N = 0, U = 0;
+        std::vector<Species> sp;
     };
     std::string out;  // <sim_dir>simulation_output/
-    std::vector<Species> sp;
+    std::vector<std::string> names;
     int diag_period = 1, phase_period = 1, device = 0;
-    int N = 0, U = 0;
     Slot slot[2];
     std::thread th;
     std::mutex mu;
@@ -577,26 +649,61 @@ struct DiagOutput {
     }
 
     void start() {
-        for (auto& s : slot) {
-            FS_CUDA(cudaHostAlloc((void**)&s.host, sizeof(double) * (3 * (size_t)N + 2 * (size_t)U), 0));
-            FS_CUDA(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
-        }
+        for (auto& s : slot) FS_CUDA(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
         th = std::thread([this] { writer(); });
     }
 
-    // Copy the state (and the reduced grid) for iteration `iter` on `st`.
-    void enqueue(cudaStream_t st, int iter, bool particles, bool reduced, const double* x, const double* p,
-                 const double* f, const double* rx, const double* re) {
+    // The files of a mesh: leaf point indices and the full panel tree.
+    static Species snapshot(const std::string& name, int start, int n, const HostMesh& M) {
+        Species q;
+        q.name = name;
+        q.start = start;
+        q.n = n;
+        q.leaf_inds.reserve(M.leaves.size() * 9);
+        for (int l : M.leaves)
+            for (int k = 0; k < 9; ++k) q.leaf_inds.push_back(M.panels[l].pts[k]);
+        q.tree.assign(8 + kTreeRecord * M.panels.size(), 0);
+        const int64_t np = (int64_t)M.panels.size();
+        std::memcpy(q.tree.data(), &np, 8);
+        for (size_t i = 0; i < M.panels.size(); ++i) {
+            const HostPanel& P = M.panels[i];
+            const int32_t v[18] = {(int32_t)i, P.level, P.parent, P.which, P.pts[0], P.pts[1], P.pts[2],
+                                   P.pts[3], P.pts[4], P.pts[5], P.pts[6], P.pts[7], P.pts[8], P.left,
+                                   P.top, P.right, P.bottom, P.child};
+            unsigned char* r = q.tree.data() + 8 + kTreeRecord * i;
+            std::memcpy(r, v, sizeof(v));
+            const int8_t b[5] = {(int8_t)(P.lb ? 1 : 0), (int8_t)(P.rb ? 1 : 0), (int8_t)(P.xp ? 1 : 0),
+                                 (int8_t)(P.pr ? 1 : 0), (int8_t)(P.needs ? 1 : 0)};
+            std::memcpy(r + sizeof(v), b, 5);
+        }
+        return q;
+    }
+
+    // Copy the state (N points) and the reduced grid (U values) for iteration
+    // `iter` on `st`; `sp` describes the species.
+    void enqueue(cudaStream_t st, int iter, bool particles, bool reduced, int N, int U, std::vector<Species> sp,
+                 const double* x, const double* p, const double* f, const double* rx, const double* re) {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait(lk, [&] { return !slot[0].busy || !slot[1].busy; });
         if (!error.empty()) fail(FS_ERR_STATE, "diagnostic output failed: " + error);
         const int k = slot[0].busy ? 1 : 0;
         Slot& S = slot[k];
         S.busy = true;
+        lk.unlock();
+        const size_t need = 3 * (size_t)N + 2 * (size_t)U;
+        if (S.cap < need) {
+            if (S.host) FS_CUDA(cudaFreeHost(S.host));
+            S.host = nullptr;
+            S.cap = 0;
+            FS_CUDA(cudaHostAlloc((void**)&S.host, sizeof(double) * std::max<size_t>(need, 1), 0));
+            S.cap = need;
+        }
         S.iter = iter;
         S.particles = particles;
         S.reduced = reduced;
-        lk.unlock();
+        S.N = N;
+        S.U = U;
+        S.sp = std::move(sp);
         const size_t n = sizeof(double) * (size_t)N, u = sizeof(double) * (size_t)U;
         if (particles) {
             FS_CUDA(cudaMemcpyAsync(S.host, x, n, cudaMemcpyDeviceToHost, st));
@@ -633,38 +740,20 @@ struct DiagOutput {
 
     void write_slot(const Slot& S) {
         const std::string it = std::to_string(S.iter);
+        const size_t N = S.N;
         if (S.particles) {
-            for (const auto& q : sp) {
+            for (const auto& q : S.sp) {
                 const std::string d = out + q.name + "/";
                 write_file(d + "xs/xs_" + it, S.host + q.start, sizeof(double) * q.n);
                 write_file(d + "ps/ps_" + it, S.host + N + q.start, sizeof(double) * q.n);
-                write_file(d + "fs/fs_" + it, S.host + 2 * (size_t)N + q.start, sizeof(double) * q.n);
-                const HostMesh& M = *q.mesh;
-                std::vector<int32_t> inds;
-                inds.reserve(M.leaves.size() * 9);
-                for (int l : M.leaves)
-                    for (int k = 0; k < 9; ++k) inds.push_back(M.panels[l].pts[k]);
-                write_file(d + "panels/leaf_point_inds_" + it, inds.data(), sizeof(int32_t) * inds.size());
-                std::vector<unsigned char> tree(8 + kTreeRecord * M.panels.size(), 0);
-                const int64_t np = (int64_t)M.panels.size();
-                std::memcpy(tree.data(), &np, 8);
-                for (size_t i = 0; i < M.panels.size(); ++i) {
-                    const HostPanel& P = M.panels[i];
-                    const int32_t v[18] = {(int32_t)i, P.level, P.parent, P.which, P.pts[0], P.pts[1], P.pts[2],
-                                           P.pts[3], P.pts[4], P.pts[5], P.pts[6], P.pts[7], P.pts[8], P.left,
-                                           P.top, P.right, P.bottom, P.child};
-                    unsigned char* r = tree.data() + 8 + kTreeRecord * i;
-                    std::memcpy(r, v, sizeof(v));
-                    const int8_t b[5] = {(int8_t)(P.lb ? 1 : 0), (int8_t)(P.rb ? 1 : 0), (int8_t)(P.xp ? 1 : 0),
-                                         (int8_t)(P.pr ? 1 : 0), (int8_t)(P.needs ? 1 : 0)};
-                    std::memcpy(r + sizeof(v), b, 5);
-                }
-                write_file(d + "panels/full_tree_" + it, tree.data(), tree.size());
+                write_file(d + "fs/fs_" + it, S.host + 2 * N + q.start, sizeof(double) * q.n);
+                write_file(d + "panels/leaf_point_inds_" + it, q.leaf_inds.data(), sizeof(int32_t) * q.leaf_inds.size());
+                write_file(d + "panels/full_tree_" + it, q.tree.data(), q.tree.size());
             }
         }
         if (S.reduced) {
-            write_file(out + "reduce_xs/xs_" + it, S.host + 3 * (size_t)N, sizeof(double) * U);
-            write_file(out + "reduced_es/es_" + it, S.host + 3 * (size_t)N + U, sizeof(double) * U);
+            write_file(out + "reduce_xs/xs_" + it, S.host + 3 * N, sizeof(double) * S.U);
+            write_file(out + "reduced_es/es_" + it, S.host + 3 * N + S.U, sizeof(double) * S.U);
         }
     }
 
@@ -762,6 +851,56 @@ struct Sim {
         }
     }
 
+    // Panel records, leaf list and leaf slots of the species' current mesh.
+    void upload_mesh(SpeciesState& ss) {
+        const HostMesh& M = ss.mesh;
+        std::vector<int> rec(M.panels.size() * 18);
+        M.panel_records(rec.data());
+        upload(ss.rec, rec);
+        upload(ss.leaves, M.leaves);
+        std::vector<int> slot(M.panels.size(), -1);
+        for (size_t l = 0; l < M.leaves.size(); ++l) slot[M.leaves[l]] = (int)l;
+        upload(ss.leaf_slot, slot);
+        ss.nleaves = (int)M.leaves.size();
+        ss.coef.ensure((size_t)ss.nleaves * 11);
+    }
+
+    // Reduced grid of a species (get_reduced_xs_ws, AMRStructure.cpp:147-185):
+    // unique x strictly increasing, point -> unique map (global, offset by
+    // ss.roff), per-unique point lists in ascending point index.  Returns the
+    // unique x.
+    std::vector<double> reduced_maps(SpeciesState& ss, const std::vector<double>& xs) {
+        const int n = ss.n;
+        std::vector<int> order(n);
+        for (int i = 0; i < n; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return xs[a] < xs[b]; });
+        std::vector<int> inv(n);
+        std::vector<double> ux;
+        double val = xs[order[0]];
+        ux.push_back(val);
+        inv[order[0]] = 0;
+        for (int k = 1; k < n; ++k) {
+            const double v = xs[order[k]];
+            if (v > val) {
+                val = v;
+                ux.push_back(v);
+            }
+            inv[order[k]] = (int)ux.size() - 1;
+        }
+        ss.nu = (int)ux.size();
+        std::vector<int> off(ss.nu + 1, 0), idx(n);
+        for (int i = 0; i < n; ++i) off[inv[i] + 1]++;
+        for (int u = 0; u < ss.nu; ++u) off[u + 1] += off[u];
+        std::vector<int> fill(off.begin(), off.end() - 1);
+        for (int i = 0; i < n; ++i) idx[fill[inv[i]]++] = i;
+        std::vector<int> inv_global(n);
+        for (int i = 0; i < n; ++i) inv_global[i] = inv[i] + ss.roff;
+        upload(ss.inv, inv_global);
+        upload(ss.col_off, off);
+        upload(ss.col_idx, idx);
+        return ux;
+    }
+
     void create(const fs_sim_params& P, cudaStream_t external = nullptr) {
         prm = P;
         if (P.num_species < 1 || P.num_species > 8) fail(FS_ERR_ARG, "num_species must be 1..8");
@@ -789,6 +928,24 @@ struct Sim {
             auto ss = std::make_unique<SpeciesState>();
             ss->mesh.build(S.initial_height, S.p_height, P.xmin, P.xmax, S.pmin, S.pmax);
             HostMesh& M = ss->mesh;
+            ss->nbase = (int)M.xs.size();
+            const double kx = 2.0 * M_PI / L * S.normalized_wavenumber;
+            // initial condition (AMRStructure ctor / generate_mesh at the initial step)
+            std::vector<double> f0(M.xs.size());
+            for (size_t i = 0; i < f0.size(); ++i)
+                f0[i] = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, M.xs[i], M.ps[i]);
+            ss->adaptive = S.do_adaptively_refine && S.n_amr_eps > 0;
+            if (ss->adaptive) {
+                if (S.n_amr_eps > 5) fail(FS_ERR_ARG, "at most 5 amr_epsilons");
+                ss->max_height = S.max_height;
+                ss->neps = S.n_amr_eps;
+                for (int k = 0; k < S.n_amr_eps; ++k) ss->eps[k] = S.amr_eps[k];
+                ss->base_mesh = M;
+                M.adapt(f0, ss->eps, ss->neps, ss->max_height,
+                        [&](const double* x, const double* p, int n, double* out) {
+                            for (int i = 0; i < n; ++i) out[i] = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, x[i], p[i]);
+                        });
+            }
             ss->start = N;
             ss->n = (int)M.xs.size();
             ss->q = S.q;
@@ -800,12 +957,11 @@ struct Sim {
             base.start[s] = N;
             base.qm[s] = ss->qm;
             N += ss->n;
-            // initial condition and weights (AMRStructure ctor / generate_mesh / set_leaves_weights)
-            const double kx = 2.0 * M_PI / L * S.normalized_wavenumber;
+            // weights (set_leaves_weights)
             std::vector<double> w0 = M.base_weights(S.q, P.quadrature);
             double fmin = 0;
             for (int i = 0; i < ss->n; ++i) {
-                const double fv = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, M.xs[i], M.ps[i]);
+                const double fv = f0[i];
                 hx.push_back(M.xs[i]);
                 hp.push_back(M.ps[i]);
                 hf.push_back(fv);
@@ -813,23 +969,17 @@ struct Sim {
                 if (i == 0 || fv < fmin) fmin = fv;
             }
             ss->f_beyond = fmin;
-            upload(ss->lat_x, M.xs);
-            upload(ss->lat_p, M.ps);
+            upload(ss->lat_x, std::vector<double>(M.xs.begin(), M.xs.begin() + ss->nbase));
+            upload(ss->lat_p, std::vector<double>(M.ps.begin(), M.ps.begin() + ss->nbase));
             upload(ss->w0, w0);
-            std::vector<int> rec(M.panels.size() * 18);
-            M.panel_records(rec.data());
-            upload(ss->rec, rec);
-            upload(ss->leaves, M.leaves);
-            std::vector<int> slot(M.panels.size(), -1);
-            for (size_t l = 0; l < M.leaves.size(); ++l) slot[M.leaves[l]] = (int)l;
-            upload(ss->leaf_slot, slot);
+            upload_mesh(*ss);
             // lattice rows (ascending p), each listing its points by column
             ss->nxl = M.nx();
             ss->npl = M.np();
             {
                 const double hx = L / ss->npx / 2, hp = (S.pmax - S.pmin) / ss->npp / 2;
                 std::vector<int> rows((size_t)ss->nxl * ss->npl, -1);
-                for (int i = 0; i < ss->n; ++i) {
+                for (int i = 0; i < ss->nbase; ++i) {
                     const int c = (int)std::lround((M.xs[i] - P.xmin) / hx);
                     const int r = (int)std::lround((M.ps[i] - S.pmin) / hp);
                     if (c < 0 || c >= ss->nxl || r < 0 || r >= ss->npl || rows[(size_t)r * ss->nxl + c] != -1)
@@ -841,46 +991,17 @@ struct Sim {
             while (ss->pow2 < ss->nxl) ss->pow2 <<= 1;
             if ((size_t)ss->pow2 * (sizeof(double) + sizeof(int)) > 200 * 1024)
                 fail(FS_ERR_UNSUPPORTED, "mesh rows longer than the row sort supports");
-            ss->sx.ensure(ss->n);
-            ss->sortx.ensure(ss->n);
-            ss->sortp.ensure(ss->n);
-            ss->order.ensure(ss->n);
-            ss->leaf_of.ensure(ss->n);
+            ss->sx.ensure(ss->nbase);
+            ss->sortx.ensure(ss->nbase);
+            ss->sortp.ensure(ss->nbase);
+            ss->order.ensure(ss->nbase);
+            ss->leaf_of.ensure(ss->nbase);
             ss->first_col.ensure(ss->npl);
             ss->walk_hist.ensure((size_t)ss->npl * kHist);
-            ss->coef.ensure((size_t)ss->nleaves * 11);
-            ss->fnew.ensure(ss->n);
-            // reduced grid of the lattice: unique x (strictly increasing, as
-            // get_reduced_xs_ws), point -> unique map, per-unique point lists
-            std::vector<int> order(ss->n);
-            for (int i = 0; i < ss->n; ++i) order[i] = i;
-            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return M.xs[a] < M.xs[b]; });
-            std::vector<int> inv(ss->n);
-            std::vector<double> ux;
-            double val = M.xs[order[0]];
-            ux.push_back(val);
-            inv[order[0]] = 0;
-            for (int k = 1; k < ss->n; ++k) {
-                const double v = M.xs[order[k]];
-                if (v > val) {
-                    val = v;
-                    ux.push_back(v);
-                }
-                inv[order[k]] = (int)ux.size() - 1;
-            }
-            ss->nu = (int)ux.size();
+            ss->fnew.ensure(ss->nbase);
             ss->roff = U;
+            const std::vector<double> ux = reduced_maps(*ss, M.xs);
             U += ss->nu;
-            std::vector<int> off(ss->nu + 1, 0), idx(ss->n);
-            for (int i = 0; i < ss->n; ++i) off[inv[i] + 1]++;
-            for (int u = 0; u < ss->nu; ++u) off[u + 1] += off[u];
-            std::vector<int> fill(off.begin(), off.end() - 1);
-            for (int i = 0; i < ss->n; ++i) idx[fill[inv[i]]++] = i;  // ascending point index per column
-            std::vector<int> inv_global(ss->n);
-            for (int i = 0; i < ss->n; ++i) inv_global[i] = inv[i] + ss->roff;
-            upload(ss->inv, inv_global);
-            upload(ss->col_off, off);
-            upload(ss->col_idx, idx);
             hrx.insert(hrx.end(), ux.begin(), ux.end());
             sp.push_back(std::move(ss));
         }
@@ -989,29 +1110,35 @@ struct Sim {
     }
 
     // AMRStructure::remesh for every species (interpolation + weights).
+    MeshView mesh_view(const SpeciesState& ss) const {
+        MeshView M;
+        M.rec = ss.rec.p;
+        M.leaf_slot = ss.leaf_slot.p;
+        M.lat_x = ss.lat_x.p;
+        M.lat_p = ss.lat_p.p;
+        M.coef = ss.coef.p;
+        M.npx = ss.npx;
+        M.npp = ss.npp;
+        M.n = ss.nbase;
+        M.xmin = prm.xmin;
+        M.pmin = ss.mesh.pmin;
+        M.Lx = L;
+        M.dxp = L / ss.npx;
+        M.dpp = (ss.mesh.pmax - ss.mesh.pmin) / ss.npp;
+        M.f_beyond = ss.f_beyond;
+        return M;
+    }
+
     void remesh_kernels() {
+        bool any_adaptive = false;
         for (auto& s : sp) {
             const int a = s->start;
+            const int nb = s->nbase;
             ProfScope prof("remesh", st);
             k_panel_fit<<<blocks(s->nleaves, 128), 128, 0, st>>>(s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a,
                                                             f.p + a, s->coef.p);
-            MeshView M;
-            M.rec = s->rec.p;
-            M.leaf_slot = s->leaf_slot.p;
-            M.lat_x = s->lat_x.p;
-            M.lat_p = s->lat_p.p;
-            M.coef = s->coef.p;
-            M.npx = s->npx;
-            M.npp = s->npp;
-            M.n = s->n;
-            M.xmin = prm.xmin;
-            M.pmin = s->mesh.pmin;
-            M.Lx = L;
-            M.dxp = L / s->npx;
-            M.dpp = (s->mesh.pmax - s->mesh.pmin) / s->npp;
-            M.f_beyond = s->f_beyond;
-            k_shift<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, L, x.p + a, p.p + a, s->sx.p,
-                                                 status.p);
+            const MeshView M = mesh_view(*s);
+            k_shift<<<blocks(nb), kT, 0, st>>>(nb, s->lat_x.p, s->lat_p.p, L, x.p + a, p.p + a, s->sx.p, status.p);
             const size_t smem = (size_t)s->pow2 * (sizeof(double) + sizeof(int));
             if (smem > 48 * 1024)
                 FS_CUDA(cudaFuncSetAttribute(k_row_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1022,12 +1149,103 @@ struct Sim {
             k_walk_rows<<<blocks(s->npl, 64), 64, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
                                                            s->sortp.p, s->first_col.p, s->leaf_of.p, s->walk_hist.p,
                                                            status.p);
-            k_eval_points<<<blocks(s->n), kT, 0, st>>>(M, s->sortx.p, s->sortp.p, s->order.p, s->leaf_of.p,
-                                                       s->fnew.p);
-            k_reset_points<<<blocks(s->n), kT, 0, st>>>(s->n, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
-                                                       p.p + a, f.p + a, qw.p + a);
+            k_eval_points<<<blocks(nb), kT, 0, st>>>(M, s->sortx.p, s->sortp.p, s->order.p, s->leaf_of.p,
+                                                     s->fnew.p);
+            if (s->adaptive) {
+                any_adaptive = true;  // f at the lattice stays in fnew; the old state is still needed
+            } else {
+                k_reset_points<<<blocks(nb), kT, 0, st>>>(nb, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
+                                                         p.p + a, f.p + a, qw.p + a);
+            }
         }
         FS_LAUNCHED(7LL * (long long)sp.size());
+        if (any_adaptive) adaptive_remesh();
+    }
+
+    // generate_mesh after a step for adaptive species (AMRStructure_amr.cpp:841-941):
+    // the lattice values from the walk, then refinement passes on the host whose
+    // new points are interpolated on the device from the previous mesh.  The
+    // point counts change, so the state is laid out again.
+    void adaptive_remesh() {
+        check_status();
+        const int ns = (int)sp.size();
+        std::vector<std::vector<double>> hx(ns), hp(ns), hf(ns), hq(ns);
+        DevBuf<double> dx, dp, df;
+        for (int k = 0; k < ns; ++k) {
+            SpeciesState& S = *sp[k];
+            const int a = S.start;
+            if (!S.adaptive) {
+                for (auto* v : {&hx[k], &hp[k], &hf[k], &hq[k]}) v->resize(S.n);
+                FS_CUDA(cudaMemcpy(hx[k].data(), x.p + a, 8 * (size_t)S.n, cudaMemcpyDeviceToHost));
+                FS_CUDA(cudaMemcpy(hp[k].data(), p.p + a, 8 * (size_t)S.n, cudaMemcpyDeviceToHost));
+                FS_CUDA(cudaMemcpy(hf[k].data(), f.p + a, 8 * (size_t)S.n, cudaMemcpyDeviceToHost));
+                FS_CUDA(cudaMemcpy(hq[k].data(), qw.p + a, 8 * (size_t)S.n, cudaMemcpyDeviceToHost));
+                continue;
+            }
+            std::vector<double> fv(S.nbase);
+            FS_CUDA(cudaMemcpy(fv.data(), S.fnew.p, 8 * (size_t)S.nbase, cudaMemcpyDeviceToHost));
+            HostMesh nm = S.base_mesh;
+            const MeshView M = mesh_view(S);
+            nm.adapt(fv, S.eps, S.neps, S.max_height, [&](const double* xs, const double* ps, int n, double* out) {
+                dx.ensure(n);
+                dp.ensure(n);
+                df.ensure(n);
+                h2d(dx.p, xs, 8 * (size_t)n);
+                h2d(dp.p, ps, 8 * (size_t)n);
+                k_interp_points<<<blocks(n), kT, 0, st>>>(M, x.p + a, p.p + a, n, dx.p, dp.p, df.p, status.p);
+                FS_LAUNCHED(1);
+                check_status();
+                FS_CUDA(cudaMemcpy(out, df.p, 8 * (size_t)n, cudaMemcpyDeviceToHost));
+            });
+            const std::vector<double> w = nm.base_weights(S.q, prm.quadrature);
+            hq[k].resize(nm.xs.size());
+            for (size_t i = 0; i < nm.xs.size(); ++i) hq[k][i] = w[i] * fv[i];
+            hx[k] = nm.xs;
+            hp[k] = nm.ps;
+            hf[k] = std::move(fv);
+            S.mesh = std::move(nm);
+            upload(S.w0, w);
+        }
+        relayout(hx, hp, hf, hq);
+    }
+
+    // Lay the species' states out again after their point counts changed.
+    void relayout(const std::vector<std::vector<double>>& hx, const std::vector<std::vector<double>>& hp,
+                  const std::vector<std::vector<double>>& hf, const std::vector<std::vector<double>>& hq) {
+        const int ns = (int)sp.size();
+        std::vector<double> ax, ap, af, aq, arx;
+        N = 0;
+        U = 0;
+        for (int k = 0; k < ns; ++k) {
+            SpeciesState& S = *sp[k];
+            S.start = N;
+            S.n = (int)hx[k].size();
+            base.start[k] = N;
+            N += S.n;
+            ax.insert(ax.end(), hx[k].begin(), hx[k].end());
+            ap.insert(ap.end(), hp[k].begin(), hp[k].end());
+            af.insert(af.end(), hf[k].begin(), hf[k].end());
+            aq.insert(aq.end(), hq[k].begin(), hq[k].end());
+            if (S.adaptive) upload_mesh(S);
+            S.roff = U;
+            const std::vector<double> ux = reduced_maps(S, hx[k]);
+            U += S.nu;
+            arx.insert(arx.end(), ux.begin(), ux.end());
+        }
+        for (int k = ns; k < 9; ++k) base.start[k] = N;
+        upload(x, ax);
+        upload(p, ap);
+        upload(f, af);
+        upload(qw, aq);
+        for (auto* b : {&e, &xkA, &xkB, &pst, &accX, &accP}) b->ensure(N);
+        base.x = x.p;
+        base.p = p.p;
+        base.pst = pst.p;
+        base.accX = accX.p;
+        base.accP = accP.p;
+        upload(rx, arx);
+        rw.ensure(U);
+        re.ensure(U);
     }
 
     void remesh() {
@@ -1100,7 +1318,12 @@ struct Sim {
         if (!out) return;
         const bool particles = iter % out->phase_period == 0;
         const bool reduced = reduced_now && iter % out->diag_period == 0;
-        if (particles || reduced) out->enqueue(st, iter, particles, reduced, x.p, p.p, f.p, rx.p, re.p);
+        if (!particles && !reduced) return;
+        std::vector<DiagOutput::Species> q;
+        if (particles)
+            for (size_t k = 0; k < sp.size(); ++k)
+                q.push_back(DiagOutput::snapshot(out->names[k], sp[k]->start, sp[k]->n, sp[k]->mesh));
+        out->enqueue(st, iter, particles, reduced, N, U, std::move(q), x.p, p.p, f.p, rx.p, re.p);
     }
 
     void set_output(const std::string& sim_dir, const std::vector<std::string>& names, int diag_period,
@@ -1112,16 +1335,8 @@ struct Sim {
         o->diag_period = diag_period;
         o->phase_period = phase_period;
         o->device = prm.device;
-        o->N = N;
-        o->U = U;
-        for (size_t k = 0; k < sp.size(); ++k) {
-            DiagOutput::Species q;
-            q.name = k < names.size() && !names[k].empty() ? names[k] : "species" + std::to_string(k);
-            q.start = sp[k]->start;
-            q.n = sp[k]->n;
-            q.mesh = &sp[k]->mesh;
-            o->sp.push_back(q);
-        }
+        for (size_t k = 0; k < sp.size(); ++k)
+            o->names.push_back(k < names.size() && !names[k].empty() ? names[k] : "species" + std::to_string(k));
         o->start();
         out = std::move(o);
         // the state as it stands (the ctor's dump at iteration 0)
@@ -1186,8 +1401,8 @@ fs_status fs_sim_remesh(fs_sim* sim) {
         FS_CUDA(cudaSetDevice(sim->impl.prm.device));
         sim->impl.remesh();
         if (sim->impl.out && sim->impl.iter % sim->impl.out->diag_period == 0)
-            sim->impl.out->enqueue(sim->impl.st, sim->impl.iter, false, true, nullptr, nullptr, nullptr,
-                                   sim->impl.rx.p, sim->impl.re.p);
+            sim->impl.out->enqueue(sim->impl.st, sim->impl.iter, false, true, sim->impl.N, sim->impl.U, {}, nullptr,
+                                   nullptr, nullptr, sim->impl.rx.p, sim->impl.re.p);
         sim->impl.check_status();
     });
 }
@@ -1243,9 +1458,9 @@ fs_status fs_sim_import_xp(fs_sim* sim, const double* xs, const double* ps, cons
         FS_CUDA(cudaSetDevice(S.prm.device));
         FS_CUDA(cudaStreamSynchronize(S.st));
         const size_t b = sizeof(double) * S.N;
-        if (xs) FS_CUDA(cudaMemcpy(S.x.p, xs, b, cudaMemcpyHostToDevice));
-        if (ps) FS_CUDA(cudaMemcpy(S.p.p, ps, b, cudaMemcpyHostToDevice));
-        if (es) FS_CUDA(cudaMemcpy(S.e.p, es, b, cudaMemcpyHostToDevice));
+        if (xs) fsb::h2d(S.x.p, xs, b);
+        if (ps) fsb::h2d(S.p.p, ps, b);
+        if (es) fsb::h2d(S.e.p, es, b);
     });
 }
 
@@ -1591,6 +1806,8 @@ struct Batch {
         for (auto& s : sims) {
             if (s->prm.field_kind != FS_FIELD_DIRECT32C && s->prm.field_kind != FS_FIELD_DIRECT64) return false;
             if (s->prm.use_external_field) return false;
+            for (const auto& q : s->sp)
+                if (q->adaptive) return false;  // point counts change at remesh
         }
         return true;
     }
@@ -1869,8 +2086,14 @@ namespace fsb {
 double estimate_sim_bytes(const fs_sim_params& P) {
     double n = 0;
     for (int s = 0; s < P.num_species && s < 8; ++s) {
-        const double h = P.species[s].initial_height, ph = P.species[s].p_height;
-        n += (2.0 * std::pow(2.0, h) + 1.0) * (2.0 * std::pow(2.0, h + ph) + 1.0);
+        const fs_species_params& S = P.species[s];
+        const double h = S.initial_height, ph = S.p_height;
+        double pts = (2.0 * std::pow(2.0, h) + 1.0) * (2.0 * std::pow(2.0, h + ph) + 1.0);
+        // adaptive refinement can split leaves up to max_height: each level at
+        // most quadruples the points (bounded at 64x)
+        if (S.do_adaptively_refine && S.n_amr_eps > 0)
+            pts *= std::min(64.0, std::pow(4.0, std::max(0, S.max_height - S.initial_height - S.p_height)));
+        n += pts;
     }
     double per_point = 1100.0;
     if (P.field_kind == FS_FIELD_TREECODE64 || P.field_kind == FS_FIELD_TREECODE32C) per_point = 1400.0;

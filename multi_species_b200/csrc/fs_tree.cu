@@ -772,6 +772,7 @@ class Treecode final : public FieldEngine {
         }
         consts_.ensure(c.size());
         FS_CUDA(cudaMemcpy(consts_.p, c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+        FS_CUDA(cudaStreamSynchronize(nullptr));  // the copy lands before the engine's non-blocking streams read it
         norm_ = std::sqrt(L * L + 4 * eps * eps) / L;
         cbg_ = 1 / std::sqrt(L * L + 4 * eps * eps);
     }

@@ -43,7 +43,9 @@ class FsoSpecies(C.Structure):
     _fields_ = [("q", C.c_double), ("m", C.c_double), ("initial_height", C.c_int),
                 ("p_height", C.c_int), ("pmin", C.c_double), ("pmax", C.c_double),
                 ("ics_type", C.c_int), ("pth", C.c_double), ("pstr", C.c_double),
-                ("amp", C.c_double), ("normalized_wavenumber", C.c_double)]
+                ("amp", C.c_double), ("normalized_wavenumber", C.c_double),
+                ("do_adaptively_refine", C.c_int), ("max_height", C.c_int), ("n_amr_eps", C.c_int),
+                ("amr_eps", C.c_double * 5)]
 
 
 class FsoSim(C.Structure):
@@ -142,6 +144,52 @@ def direct_sum(L, eps, targets, sources, q):
     es = np.zeros(len(t))
     lib().fso_direct_sum(L, eps, es, t, len(t), s, q, len(s))
     return es
+
+
+def adaptive_mesh(h, ph, xmin, xmax, pmin, pmax, f0_params, amr_eps, max_height, L=None):
+    """Initial adaptive mesh: the uniform mesh, f0 at its points, then
+    generate_mesh's refinement with f0 at the new points.  f0_params =
+    (ics_type, pth, pstr, amp, normalized_wavenumber).  Returns (xs, ps, f,
+    panels (n x 18), leaves)."""
+    m = Mesh(h, ph, xmin, xmax, pmin, pmax)
+    ics, pth, pstr, amp, nk = f0_params
+    kx = 2 * np.pi / ((xmax - xmin) if L is None else L) * nk
+    n = m.npoints
+    f = np.array([lib().fso_f0(ics, pth, pstr, kx, amp, x, p) for x, p in zip(m.xs, m.ps)])
+    fbuf = lib().fso_f0  # keep a reference while the callback runs
+    CB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int,
+                     C.POINTER(C.c_double))
+
+    def cb(ctx, xp, pp, k, out):
+        for i in range(k):
+            out[i] = fbuf(ics, pth, pstr, kx, amp, xp[i], pp[i])
+
+    ccb = CB(cb)
+    L_ = lib()
+    L_.fso_mesh_adapt.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int, CB, C.c_void_p]
+    L_.fso_mesh_adapt.restype = C.c_void_p
+    L_.malloc_double = None
+    import ctypes.util
+    libc = C.CDLL(ctypes.util.find_library("c"))
+    libc.malloc.restype = C.c_void_p
+    libc.malloc.argtypes = [C.c_size_t]
+    libc.free.argtypes = [C.c_void_p]
+    buf = libc.malloc(8 * n)
+    C.memmove(buf, f.ctypes.data, 8 * n)
+    e = (C.c_double * 5)(*amr_eps[:5])
+    fp = L_.fso_mesh_adapt(m._m, buf, e, len(amr_eps[:5]), max_height, ccb, None)
+    m.npoints = L_.fso_mesh_npoints(m._m)
+    m.npanels = L_.fso_mesh_npanels(m._m)
+    m.nleaves = L_.fso_mesh_nleaves(m._m)
+    xs, ps = np.zeros(m.npoints), np.zeros(m.npoints)
+    L_.fso_mesh_points(m._m, xs, ps)
+    panels = np.zeros((m.npanels, PANEL_INTS), dtype=np.int32)
+    L_.fso_mesh_panels(m._m, panels)
+    leaves = np.zeros(m.nleaves, dtype=np.int32)
+    L_.fso_mesh_leaves(m._m, leaves)
+    fo = np.ctypeslib.as_array((C.c_double * m.npoints).from_address(fp)).copy()
+    libc.free(fp)
+    return xs, ps, fo, panels, leaves
 
 
 def direct_sum_open(eps, targets, sources, q):
@@ -254,6 +302,15 @@ def reduce(xs, q):
 
 
 # ---------------------------------------------------------------- simulation
+def _amr_params(sp: dict):
+    """(do_adaptively_refine, max_height, amr_epsilons) as AMRSimulation_load.cpp:246-258
+    reads them: without amr_epsilons the refinement is disabled."""
+    eps = sp.get("amr_epsilons")
+    on = bool(sp.get("do_adaptively_refine", False)) and eps is not None
+    eps = [float(e) for e in (eps or [])][:5]
+    return (1 if on else 0), int(sp.get("max_height", sp.get("initial_height", 6))), eps
+
+
 def sim_params(deck: dict) -> FsoSim:
     """Deck dict (deck.json keys) -> oracle simulation parameters."""
     P = FsoSim()
@@ -276,6 +333,10 @@ def sim_params(deck: dict) -> FsoSim:
         S.ics_type = int(sp.get("ics_type", 1))
         S.pth, S.pstr, S.amp = sp.get("pth", 1.0), sp.get("pstr", 0.0), sp.get("amp", 0.0)
         S.normalized_wavenumber = sp.get("normalized_wavenumber", 1.0)
+        amr = _amr_params(sp)
+        S.do_adaptively_refine, S.max_height, S.n_amr_eps = amr[0], amr[1], len(amr[2])
+        for k, e in enumerate(amr[2]):
+            S.amr_eps[k] = e
     ext = deck.get("external_field") or {}
     P.use_external_field = 1 if int(ext.get("use_external_field", 0)) > 0 else 0
     if P.use_external_field:
@@ -306,6 +367,7 @@ class Sim:
         return lib().fso_sim_iter(self._s)
 
     def state(self):
+        self.n = lib().fso_sim_total_points(self._s)  # adaptive meshes change it at remesh
         a = {k: np.zeros(self.n) for k in ("xs", "ps", "fs", "q_ws", "es")}
         lib().fso_sim_state(self._s, *(a[k].ctypes.data for k in ("xs", "ps", "fs", "q_ws", "es")))
         return a

@@ -820,15 +820,32 @@ static void merge_sort(int* v, int* tmp, int n) {
     memcpy(v, tmp, sizeof(int) * n);
 }
 
+static int remesh_interp_impl(const fso_mesh* old_m, const fso_mesh* m, const double* old_xs,
+                              const double* old_ps, const double* old_fs, double f_beyond, double* new_fs,
+                              int* leaf_of_point, double* final_x);
+
 int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old_ps,
                       const double* old_fs, double f_beyond, double* new_fs,
                       int* leaf_of_point, double* final_x) {
+    return remesh_interp_impl(m, m, old_xs, old_ps, old_fs, f_beyond, new_fs, leaf_of_point, final_x);
+}
+
+int fso_remesh_interp2(const fso_mesh* old_m, const fso_mesh* new_m, const double* old_xs, const double* old_ps,
+                       const double* old_fs, double f_beyond, double* new_fs) {
+    return remesh_interp_impl(old_m, new_m, old_xs, old_ps, old_fs, f_beyond, new_fs, NULL, NULL);
+}
+
+/* old_m: panels of the previous mesh (positions old_xs/old_ps); m: the new
+ * uniform mesh whose points are located. */
+static int remesh_interp_impl(const fso_mesh* old_m, const fso_mesh* m, const double* old_xs,
+                              const double* old_ps, const double* old_fs, double f_beyond, double* new_fs,
+                              int* leaf_of_point, double* final_x) {
     const int N = m->npts;
     const double Lx = m->xmax - m->xmin;
     const int npx = 1 << m->h, npp = 1 << (m->h + m->ph);
     const int nx = 2 * npx + 1, np = 2 * npp + 1;
     const double initial_dp = (m->pmax - m->pmin) / npp;
-    locate_ctx c = {m, old_xs, old_ps, Lx};
+    locate_ctx c = {old_m, old_xs, old_ps, Lx};
     /* shift_xs (AMRStructure_interp.cpp:429-491) */
     double* sx = (double*)malloc(sizeof(double) * N);
     const double x_bl = old_xs[0], p_bl = old_ps[0], x_tl = old_xs[2], p_tl = old_ps[2];
@@ -893,7 +910,7 @@ int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old
         const int l = leaf[k];
         if (l == 0) v = f_beyond;
         else {
-            const opanel* P = &m->p[l];
+            const opanel* P = &old_m->p[l];
             double px[9], pp[9], pf[9];
             for (int i = 0; i < 9; ++i) { px[i] = old_xs[P->pts[i]]; pp[i] = old_ps[P->pts[i]]; pf[i] = old_fs[P->pts[i]]; }
             fso_panel_fit(px, pp, pf, 1, &sortx[k], &sortp[k], &v);
@@ -904,6 +921,110 @@ int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old
     }
     free(sx); free(order); free(sortx); free(sortp); free(leaf);
     return 0;
+}
+
+/* ======================================================================= */
+/* Adaptive refinement                                                      */
+/* ======================================================================= */
+/* 9-point fit coefficients (the same LU as fso_panel_fit). */
+static void fit_coefs(const double* px, const double* pp, const double* pf, double* c) {
+    double A[9][9], pdx[9], pdp[9];
+    for (int i = 0; i < 9; ++i) { pdx[i] = px[i] - px[4]; pdp[i] = pp[i] - pp[4]; }
+    for (int i = 0; i < 9; ++i) {
+        A[i][0] = 1; A[i][1] = pdx[i];
+        A[i][2] = pdx[i] * pdp[i];
+        A[i][3] = pdp[i];
+        A[i][4] = pdx[i] * pdx[i];
+        A[i][5] = pdx[i] * pdx[i] * pdp[i];
+        A[i][6] = pdx[i] * pdx[i] * pdp[i] * pdp[i];
+        A[i][7] = pdx[i] * pdp[i] * pdp[i];
+        A[i][8] = pdp[i] * pdp[i];
+        c[i] = pf[i];
+    }
+    lu_solve9(A, c);
+}
+
+double fso_interp_point(const fso_mesh* old_m, const double* old_xs, const double* old_ps, const double* old_fs,
+                        double f_beyond, double x, double p, int* rc) {
+    const double Lx = old_m->xmax - old_m->xmin;
+    /* shift_xs for one point (:429-491) */
+    const double x_bl = old_xs[0], p_bl = old_ps[0], x_tl = old_xs[2], p_tl = old_ps[2];
+    const double x_br = old_xs[6], p_br = old_ps[6], x_tr = old_xs[8], p_tr = old_ps[8];
+    double xt = x;
+    int cnt = 0;
+    while (!((x_tl - x_bl) * (p - p_bl) <= (p_tl - p_bl) * (xt - x_bl))) {
+        xt += Lx;
+        if (++cnt > 10) { *rc = -1; return 0.0; }
+    }
+    cnt = 0;
+    while (!((x_tr - x_br) * (p - p_br) > (p_tr - p_br) * (xt - (x_br)))) {
+        xt -= Lx;
+        if (++cnt > 10) { *rc = -1; return 0.0; }
+    }
+    locate_ctx c = {old_m, old_xs, old_ps, Lx};
+    int beyond = 0;
+    const int l = find_recursive(&c, &xt, p, &beyond, 0);
+    if (beyond || l == 0) return f_beyond;
+    const opanel* P = &old_m->p[l];
+    double px[9], pp[9], pf[9], k[9];
+    for (int i = 0; i < 9; ++i) { px[i] = old_xs[P->pts[i]]; pp[i] = old_ps[P->pts[i]]; pf[i] = old_fs[P->pts[i]]; }
+    fit_coefs(px, pp, pf, k);
+    const double dx = xt - px[4], dp = p - pp[4];
+    /* interpolate_from_panel's single-point expression (:1086-1088) */
+    return k[0] + k[1] * dx + k[2] * dx * dp + k[3] * dp + k[4] * dx * dx + k[5] * dx * dx * dp +
+           k[6] * dx * dx * dp * dp + k[7] * dx * dp * dp + k[8] * dp * dp;
+}
+
+/* test_panel (AMRStructure_amr.cpp:971-1081).  The p-derivative criterion of
+ * the reference reads six entries of which it sets two (:1051-1061, the rest
+ * are uninitialised); the restatement uses the two it sets. */
+static void amr_test(fso_mesh* m, int pi, const double* f, const double* eps, int neps, int max_height) {
+    opanel* P = &m->p[pi];
+    double pf[9];
+    for (int i = 0; i < 9; ++i) pf[i] = f[P->pts[i]];
+    int crit = 0;
+    if (neps > 0) {
+        double mx = pf[0], mn = pf[0];
+        for (int i = 1; i < 9; ++i) { if (mx < pf[i]) mx = pf[i]; if (mn > pf[i]) mn = pf[i]; }
+        crit = crit || (mx - mn > eps[0]);
+        if (neps > 1) crit = crit || (mx - mn) / pf[4] > eps[1];
+        if (neps > 2) crit = crit || mx / mn > eps[2];
+    }
+    if (neps > 3) {
+        const double dx = m->xs[P->pts[3]] - m->xs[P->pts[0]];
+        double md = fabs((pf[3] - pf[0]) / dx);
+        for (int i = 1; i < 6; ++i) { double v = fabs((pf[3 + i] - pf[i]) / dx); if (md < v) md = v; }
+        crit = crit || (md > eps[3]);
+    }
+    if (neps > 4) {
+        const double dp = m->ps[P->pts[1]] - m->ps[P->pts[0]];
+        double a[2] = {0.0, 0.0};
+        for (int jj = 0; jj < 3; ++jj)
+            for (int ii = 0; ii < 2; ++ii) a[ii] = fabs((pf[3 * jj + ii + 1] - pf[3 * jj + ii]) / dp);
+        const double md = a[0] < a[1] ? a[1] : a[0];
+        crit = crit || (md > eps[4]);
+    }
+    if (P->level < max_height && crit) { P->needs = 1; m->need_further = 1; }
+}
+
+double* fso_mesh_adapt(fso_mesh* m, double* f, const double* eps, int neps, int max_height, fso_eval_fn eval,
+                       void* ctx) {
+    m->need_further = 0;
+    for (int i = m->min_unrefined; i < m->np; ++i) amr_test(m, i, f, eps, neps, max_height);
+    while (m->need_further) {
+        m->need_further = 0;
+        const int n0 = m->npts;
+        mesh_refine_xp(m);
+        f = (double*)realloc(f, sizeof(double) * (m->npts > 0 ? m->npts : 1));
+        if (m->npts > n0) eval(ctx, m->xs + n0, m->ps + n0, m->npts - n0, f + n0);
+        for (int i = m->min_unrefined; i < m->np; ++i)
+            if (!m->p[i].xp) amr_test(m, i, f, eps, neps, max_height);
+    }
+    free(m->leaves);
+    m->leaves = (int*)malloc(sizeof(int) * m->np);
+    m->nleaves = 0;
+    mesh_collect_leaves(m, 0);
+    return f;
 }
 
 /* ======================================================================= */
@@ -1028,16 +1149,45 @@ static void sim_reduced_field(fso_sim* s) {
     free(rx); free(rw); free(inv); free(re);
 }
 
+typedef struct { const fso_species_params* q; double kx; } f0_ctx;
+static void eval_f0(void* ctx, const double* x, const double* p, int n, double* out) {
+    const f0_ctx* c = (const f0_ctx*)ctx;
+    for (int i = 0; i < n; ++i) out[i] = fso_f0(c->q->ics_type, c->q->pth, c->q->pstr, c->kx, c->q->amp, x[i], p[i]);
+}
+typedef struct {
+    const fso_mesh* old_m;
+    const double *ox, *op, *of;
+    double f_beyond;
+    int rc;
+} interp_ctx;
+static void eval_interp(void* ctx, const double* x, const double* p, int n, double* out) {
+    interp_ctx* c = (interp_ctx*)ctx;
+    for (int i = 0; i < n; ++i) {
+        int rc = 0;
+        out[i] = fso_interp_point(c->old_m, c->ox, c->op, c->of, c->f_beyond, x[i], p[i], &rc);
+        if (rc) c->rc = rc;
+    }
+}
+
 fso_sim* fso_sim_create(const fso_sim_params* prm) {
     if (prm->num_species < 1 || prm->num_species > 8) return NULL;
     fso_sim* s = (fso_sim*)calloc(1, sizeof(fso_sim));
     s->prm = *prm;
     s->Lx = prm->xmax - prm->xmin;
     int tot = 0;
+    double* f_init[8] = {0};
     for (int sp = 0; sp < prm->num_species; ++sp) {
         const fso_species_params* q = &prm->species[sp];
         s->mesh[sp] = fso_mesh_build(q->initial_height, q->p_height, prm->xmin, prm->xmax, q->pmin, q->pmax);
         if (!s->mesh[sp]) { fso_sim_destroy(s); return NULL; }
+        if (q->do_adaptively_refine && q->n_amr_eps > 0) {
+            /* generate_mesh at the initial step: f0 at every point, new ones included */
+            fso_mesh* m = s->mesh[sp];
+            f0_ctx fc = {q, 2.0 * M_PI / s->Lx * q->normalized_wavenumber};
+            double* f = (double*)malloc(sizeof(double) * m->npts);
+            eval_f0(&fc, m->xs, m->ps, m->npts, f);
+            f_init[sp] = fso_mesh_adapt(m, f, q->amr_eps, q->n_amr_eps, q->max_height, eval_f0, &fc);
+        }
         s->start[sp] = tot;
         tot += s->mesh[sp]->npts;
     }
@@ -1061,10 +1211,12 @@ fso_sim* fso_sim_create(const fso_sim_params* prm) {
         for (int i = 0; i < m->npts; ++i) {
             s->xs[a + i] = m->xs[i];
             s->ps[a + i] = m->ps[i];
-            s->fs[a + i] = fso_f0(q->ics_type, q->pth, q->pstr, kx, q->amp, m->xs[i], m->ps[i]);
+            s->fs[a + i] = f_init[sp] ? f_init[sp][i]
+                                      : fso_f0(q->ics_type, q->pth, q->pstr, kx, q->amp, m->xs[i], m->ps[i]);
             s->qws[a + i] = s->w0[sp][i] * s->fs[a + i];
             if (i == 0 || s->fs[a + i] < fmin) fmin = s->fs[a + i];
         }
+        free(f_init[sp]);
         s->f_beyond[sp] = fmin;  /* AMRStructure.cpp:124 */
     }
     sim_reduced_field(s);
@@ -1128,19 +1280,65 @@ static void sim_rk4(fso_sim* s) {
 /* AMRSimulation::remesh (src/simulation_files/AMRSimulation_remesh.cpp:3-48)
  * with AMRStructure::remesh (AMRStructure_amr.cpp:1156-1202). */
 static int sim_remesh(fso_sim* s) {
-    for (int sp = 0; sp < s->prm.num_species; ++sp) {
-        const fso_mesh* m = s->mesh[sp];
-        const int a = s->start[sp], n = m->npts;
-        double* nf = (double*)malloc(sizeof(double) * n);
-        int rc = fso_remesh_interp(m, s->xs + a, s->ps + a, s->fs + a, s->f_beyond[sp], nf, NULL, NULL);
-        if (rc) { free(nf); return rc; }
-        for (int i = 0; i < n; ++i) {
-            s->xs[a + i] = m->xs[i];
-            s->ps[a + i] = m->ps[i];
-            s->fs[a + i] = nf[i];
-            s->qws[a + i] = s->w0[sp][i] * nf[i];
+    const int ns = s->prm.num_species;
+    double *nx[8], *np_[8], *nf[8], *nq[8];
+    int cnt[8];
+    int rc = 0;
+    for (int sp = 0; sp < ns; ++sp) {
+        const fso_species_params* q = &s->prm.species[sp];
+        fso_mesh* m = s->mesh[sp];
+        const int a = s->start[sp];
+        if (q->do_adaptively_refine && q->n_amr_eps > 0) {
+            /* generate_mesh after a step: the uniform base mesh, f interpolated
+             * at its lattice, then adaptive refinement with interpolate_from_mesh */
+            fso_mesh* nm = fso_mesh_build(q->initial_height, q->p_height, s->prm.xmin, s->prm.xmax, q->pmin, q->pmax);
+            double* f = (double*)malloc(sizeof(double) * nm->npts);
+            rc = fso_remesh_interp2(m, nm, s->xs + a, s->ps + a, s->fs + a, s->f_beyond[sp], f);
+            if (rc) { free(f); fso_mesh_destroy(nm); break; }
+            interp_ctx ic = {m, s->xs + a, s->ps + a, s->fs + a, s->f_beyond[sp], 0};
+            f = fso_mesh_adapt(nm, f, q->amr_eps, q->n_amr_eps, q->max_height, eval_interp, &ic);
+            if (ic.rc) { free(f); fso_mesh_destroy(nm); rc = ic.rc; break; }
+            free(s->w0[sp]);
+            s->w0[sp] = (double*)malloc(sizeof(double) * nm->npts);
+            fso_mesh_base_weights(nm, q->q, s->prm.quadrature, s->w0[sp]);
+            fso_mesh_destroy(m);
+            s->mesh[sp] = nm;
+            m = nm;
+            nf[sp] = f;
+        } else {
+            nf[sp] = (double*)malloc(sizeof(double) * m->npts);
+            rc = fso_remesh_interp(m, s->xs + a, s->ps + a, s->fs + a, s->f_beyond[sp], nf[sp], NULL, NULL);
+            if (rc) { free(nf[sp]); break; }
         }
-        free(nf);
+        cnt[sp] = m->npts;
+        nx[sp] = (double*)malloc(sizeof(double) * cnt[sp]);
+        np_[sp] = (double*)malloc(sizeof(double) * cnt[sp]);
+        nq[sp] = (double*)malloc(sizeof(double) * cnt[sp]);
+        for (int i = 0; i < cnt[sp]; ++i) {
+            nx[sp][i] = m->xs[i];
+            np_[sp][i] = m->ps[i];
+            nq[sp][i] = s->w0[sp][i] * nf[sp][i];
+        }
+    }
+    if (rc) return rc;  /* (the partial buffers are released with the failed run) */
+    /* relayout: species concatenated in deck order */
+    int tot = 0;
+    for (int sp = 0; sp < ns; ++sp) { s->start[sp] = tot; tot += cnt[sp]; }
+    s->start[ns] = tot;
+    s->N = tot;
+    free(s->xs); free(s->ps); free(s->fs); free(s->qws); free(s->es);
+    s->xs = (double*)malloc(sizeof(double) * tot);
+    s->ps = (double*)malloc(sizeof(double) * tot);
+    s->fs = (double*)malloc(sizeof(double) * tot);
+    s->qws = (double*)malloc(sizeof(double) * tot);
+    s->es = (double*)calloc(tot, sizeof(double));
+    for (int sp = 0; sp < ns; ++sp) {
+        const int a = s->start[sp];
+        memcpy(s->xs + a, nx[sp], sizeof(double) * cnt[sp]);
+        memcpy(s->ps + a, np_[sp], sizeof(double) * cnt[sp]);
+        memcpy(s->fs + a, nf[sp], sizeof(double) * cnt[sp]);
+        memcpy(s->qws + a, nq[sp], sizeof(double) * cnt[sp]);
+        free(nx[sp]); free(np_[sp]); free(nf[sp]); free(nq[sp]);
     }
     sim_reduced_field(s);
     return 0;

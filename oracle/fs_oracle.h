@@ -69,6 +69,24 @@ double fso_f0(int ics_type, double pth, double pstr, double k, double amp, doubl
 int fso_remesh_interp(const fso_mesh* m, const double* old_xs, const double* old_ps,
                       const double* old_fs, double f_beyond, double* new_fs,
                       int* leaf_of_point, double* final_x);
+/* The same with the previous mesh's panels (old_m) distinct from the new base
+ * mesh (new_m, uniform), as after an adaptive step: f at new_m's points. */
+int fso_remesh_interp2(const fso_mesh* old_m, const fso_mesh* new_m, const double* old_xs, const double* old_ps,
+                       const double* old_fs, double f_beyond, double* new_fs);
+/* interpolate_from_mesh (AMRStructure_interp.cpp:1094-1143): f at one point from
+ * the previous mesh -- shift_xs, the recursive search from the root, the leaf's
+ * fit (f_beyond beyond the p-boundary).  *rc = -1 when shifting fails. */
+double fso_interp_point(const fso_mesh* old_m, const double* old_xs, const double* old_ps, const double* old_fs,
+                        double f_beyond, double x, double p, int* rc);
+
+/* Adaptive refinement (generate_mesh, AMRStructure_amr.cpp:901-941; test_panel
+ * :971-1081; refine_panels :506-839 on flagged panels).  f holds the values at
+ * the mesh's current points; new points get theirs from eval(ctx, x, p, n, out).
+ * Panels below max_height whose 9 values meet a criterion are split 2x2 until
+ * none is flagged.  Returns the new f (realloc'ed, npoints entries). */
+typedef void (*fso_eval_fn)(void* ctx, const double* x, const double* p, int n, double* out);
+double* fso_mesh_adapt(fso_mesh* m, double* f, const double* amr_eps, int neps, int max_height, fso_eval_fn eval,
+                       void* ctx);
 /* One 9-point biquadratic fit evaluated at (dx, dp) offsets from point 4. */
 void fso_panel_fit(const double* px, const double* py, const double* pf, int npts,
                    const double* x, const double* p, double* out);
@@ -98,6 +116,11 @@ typedef struct {
     double pmin, pmax;
     int ics_type;
     double pth, pstr, amp, normalized_wavenumber;
+    /* adaptive refinement (AMRSimulation_load.cpp:246-258) */
+    int do_adaptively_refine;
+    int max_height;
+    int n_amr_eps;              /* 0..5 */
+    double amr_eps[5];
 } fso_species_params;
 
 typedef struct {

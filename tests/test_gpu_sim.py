@@ -175,3 +175,46 @@ def test_drive_field_fp32c_session():
     drive = O.external_field(1, 0.4, 0.2, 0.37, np.zeros(len(st["xs"])), st["xs"], 3 * d["dt"])
     assert np.max(np.abs(drive)) > 1e-3
     assert rel(st["es"] - drive, field) < 1e-6
+
+
+def _adaptive_two_stream(steps=6, remesh_period=3):
+    d = decks.two_stream(h=4, ph=1, steps=steps, remesh_period=remesh_period)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=7, amr_epsilons=[0.02])
+    return d
+
+
+def test_adaptive_initial_mesh_bit_identical_to_oracle():
+    """generate_mesh at the initial step with adaptive refinement: f0 on the
+    uniform mesh, panels whose f spread exceeds 0.02 split 2x2 up to level 7."""
+    d = _adaptive_two_stream()
+    g, o = M.Simulation(d, "direct64"), O.Sim(d)
+    a, b = g.state(), o.state()
+    assert len(a["xs"]) == len(b["xs"]) > 33 * 65
+    for k in ("xs", "ps", "fs", "q_ws", "es"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_adaptive_remesh_matches_oracle():
+    """Remesh with adaptive refinement: the lattice interpolated by the walk,
+    refinement passes whose new points are interpolated from the previous mesh
+    (root search + fit), the state laid out again with the new point count."""
+    d = _adaptive_two_stream(steps=7, remesh_period=3)
+    g, o = M.Simulation(d, "direct64"), O.Sim(d)
+    for step in range(7):
+        g.step()
+        o.step()
+        a, b = g.state(), o.state()
+        assert len(a["xs"]) == len(b["xs"]), step
+        assert np.array_equal(a["xs"], b["xs"]) or rel(a["xs"], b["xs"]) < 1e-12, step
+        assert rel(a["fs"], b["fs"]) < 1e-11, step
+        assert rel(a["es"], b["es"]) < 1e-10, step
+
+
+def test_adaptive_fp32c_session_runs_with_refinement():
+    d = _adaptive_two_stream(steps=6, remesh_period=3)
+    g64, g32 = M.Simulation(d, "direct64"), M.Simulation(d, "direct32c")
+    g64.step(4)
+    g32.step(4)
+    a, b = g32.state(), g64.state()
+    assert len(a["xs"]) == len(b["xs"])
+    assert rel(a["es"], b["es"]) < 1e-5
