@@ -171,3 +171,25 @@ def test_profile_counts_graph_replayed_launches():
     assert n == 16 and ms > 0
     assert w == pytest.approx(b.pair_count(), rel=1e-12)
     b.close()
+
+
+def test_adaptive_member_alone_and_in_batch_bit_identical():
+    """A member whose mesh refines adaptively (its point count changes at each
+    remesh) steps in a batch exactly as alone; the batch is not graph-captured."""
+    ad = decks.two_stream(h=4, ph=1, steps=7, remesh_period=3)
+    ad["species_list"][0].update(do_adaptively_refine=True, max_height=6, amr_epsilons=[0.05])
+    other = _small_decks(1, seed=53)[0]
+    b1 = fs.Batch(tuning=(4, 16))
+    i1 = b1.add(ad)
+    b1.step(7)
+    alone = b1.state(i1)
+    b2 = fs.Batch(tuning=(4, 16))
+    i2 = b2.add(ad)
+    b2.add(other)
+    b2.step(7)
+    mixed = b2.state(i2)
+    assert b2.stats()["graph_steps"] == 0
+    for k in alone:
+        assert np.array_equal(alone[k], mixed[k]), k
+    b1.close()
+    b2.close()

@@ -83,3 +83,27 @@ def test_dump_errors_are_reported(tmp_path):
     with pytest.raises(M.FsError):
         g.flush_output()
     g.close()
+
+
+def test_dumps_follow_adaptive_meshes(tmp_path):
+    """With adaptive refinement the point count changes at each remesh; each
+    dump carries the mesh and the sizes of its own iteration."""
+    d = decks.two_stream(h=4, ph=1, steps=6, remesh_period=3)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=6, amr_epsilons=[0.05])
+    g = M.Simulation(d, "direct64")
+    g.set_output(str(tmp_path), diag_period=3, diag_phase_space_period=3)
+    sizes = {0: g.state()["xs"].size}
+    for it in range(1, 7):
+        g.step()
+        if it % 3 == 0:
+            sizes[it] = g.state()["xs"].size
+    g.flush_output()
+    out = tmp_path / "simulation_output" / d["species_list"][0]["name"]
+    for it, n in sizes.items():
+        assert _read(out / "xs" / f"xs_{it}").size == n
+        tree = (out / "panels" / f"full_tree_{it}").read_bytes()
+        npan = int(np.frombuffer(tree[:8], dtype=np.int64)[0])
+        assert len(tree) == 8 + 80 * npan
+        inds = _read(out / "panels" / f"leaf_point_inds_{it}", np.int32)
+        assert inds.max() == n - 1
+    g.close()
