@@ -290,6 +290,16 @@ fs_status fs_pool_estimate_bytes(const fs_sim_params* params, double* bytes);
  * species1, ...) name the directories.  Directories are created as needed. */
 fs_status fs_sim_set_output(fs_sim* sim, const char* sim_dir, const char* const* species_names, int diag_period,
                             int diag_phase_space_period);
+/* Restart from the files of iteration `iter` under <sim_dir>simulation_output/
+ * (the reference's restart, AMRSimulation.cpp:65-84 and AMRStructure_restart.cpp:
+ * 101-229): per species xs/ps/fs and full_tree; weights from the loaded leaves
+ * at the loaded positions, as the reference computes them (so a restart
+ * continues a run exactly from a dump taken right after a remesh),
+ * t = iter * dt, then the reduced-grid field on the loaded state.  The session
+ * must come from the same deck (a uniform species must load its mesh's point
+ * count).  Missing or malformed files return FS_ERR_ARG and leave the session
+ * as it was. */
+fs_status fs_sim_restart(fs_sim* sim, const char* sim_dir, const char* const* species_names, int iter);
 /* Wait until every queued file is written; FS_ERR_STATE if a write failed. */
 fs_status fs_sim_flush_output(fs_sim* sim);
 

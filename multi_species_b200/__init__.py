@@ -45,7 +45,7 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
            "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
            "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes", "fs_sim_set_output",
-           "fs_sim_flush_output"]
+           "fs_sim_flush_output", "fs_sim_restart"]
 
 
 class FsError(RuntimeError):
@@ -130,6 +130,8 @@ def lib():
         L.fs_sim_set_output.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int, C.c_int]
         L.fs_sim_set_output.restype = st
         L.fs_sim_flush_output.argtypes = [C.c_void_p]
+        L.fs_sim_restart.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int]
+        L.fs_sim_restart.restype = st
         L.fs_sim_flush_output.restype = st
         L.fs_profile_enable.argtypes = [C.c_int]
         L.fs_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), _dp, _dp]
@@ -383,6 +385,14 @@ class Simulation:
 
     def flush_output(self) -> None:
         _check(lib().fs_sim_flush_output(self._h))
+
+    def restart(self, sim_dir: str, iteration: int) -> None:
+        """Load the dump of `iteration` under sim_dir/simulation_output/ (the
+        reference's restart): the state, the panel trees, t = iteration * dt,
+        and the reduced-grid field on the loaded state."""
+        names = [str(sp.get("name", f"species{i}")).encode() for i, sp in enumerate(self.deck["species_list"])]
+        arr = (C.c_char_p * len(names))(*names)
+        _check(lib().fs_sim_restart(self._h, str(sim_dir).encode(), arr, int(iteration)))
 
     def step(self, n: int = 1) -> None:
         """n x AMRSimulation::step (AMRSimulation_step.cpp:5-99)."""

@@ -155,6 +155,8 @@ struct HostMesh {
     // gives f at new points.
     void adapt(std::vector<double>& f, const double* eps, int neps, int max_height,
                const std::function<void(const double*, const double*, int, double*)>& eval);
+    // Leaves (DFS order) of panels loaded from a restart file.
+    void restart_leaves();
     std::vector<double> base_weights(double q, int quadrature) const;
     void panel_records(int* out) const;  // 18 ints per panel
     int nx() const { return 2 * (1 << h) + 1; }

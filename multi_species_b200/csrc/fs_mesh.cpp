@@ -405,6 +405,11 @@ bool test_panel(HostMesh& m, int pi, const std::vector<double>& f, const double*
 
 }  // namespace
 
+void HostMesh::restart_leaves() {
+    leaves.clear();
+    collect_leaves(*this, 0, leaves);
+}
+
 void HostMesh::adapt(std::vector<double>& f, const double* eps, int neps, int max_height,
                      const std::function<void(const double*, const double*, int, double*)>& eval) {
     Refiner R(*this);

@@ -1253,6 +1253,111 @@ struct Sim {
         reduced_field();
     }
 
+    // Restart from the dump files of iteration `it` (AMRSimulation.cpp:65-84,
+    // AMRStructure::load_restart, AMRStructure_restart.cpp:101-229): per species
+    // xs/ps/fs and the full panel tree; weights from the loaded leaves at the
+    // loaded positions (set_leaves_weights, as the reference does: equal to the
+    // carried weights only for a dump taken right after a remesh), t = it * dt,
+    // then the reduced-grid field on the loaded state.
+    void restart(const std::string& sim_dir, const std::vector<std::string>& names, int it) {
+        if (it < 0) fail(FS_ERR_ARG, "restart iteration must be >= 0");
+        const std::string out = sim_dir + ((sim_dir.empty() || sim_dir.back() == '/') ? "" : "/") + "simulation_output/";
+        const int ns = (int)sp.size();
+        std::vector<std::vector<double>> hx(ns), hp(ns), hf(ns), hq(ns);
+        std::vector<HostMesh> meshes(ns);
+        auto read_all = [](const std::string& path) {
+            std::ifstream in(path, std::ios::in | std::ios::binary | std::ios::ate);
+            if (!in) fail(FS_ERR_ARG, "unable to open " + path);
+            const std::streamsize n = in.tellg();
+            std::vector<unsigned char> b(n > 0 ? (size_t)n : 0);
+            in.seekg(0);
+            if (n > 0) in.read(reinterpret_cast<char*>(b.data()), n);
+            if (!in) fail(FS_ERR_ARG, "error reading " + path);
+            return b;
+        };
+        auto doubles = [&](const std::string& path) {
+            const std::vector<unsigned char> b = read_all(path);
+            if (b.size() % sizeof(double)) fail(FS_ERR_ARG, "bad file size for " + path);
+            std::vector<double> v(b.size() / sizeof(double));
+            if (!v.empty()) std::memcpy(v.data(), b.data(), b.size());
+            return v;
+        };
+        for (int k = 0; k < ns; ++k) {
+            SpeciesState& S = *sp[k];
+            const std::string name = k < (int)names.size() && !names[k].empty() ? names[k] : "species" + std::to_string(k);
+            const std::string d = out + name + "/";
+            const std::string its = std::to_string(it);
+            hx[k] = doubles(d + "xs/xs_" + its);
+            hp[k] = doubles(d + "ps/ps_" + its);
+            hf[k] = doubles(d + "fs/fs_" + its);
+            if (hx[k].size() != hp[k].size() || hp[k].size() != hf[k].size() || hx[k].empty())
+                fail(FS_ERR_ARG, "mismatched xs/ps/fs sizes in the restart files of " + name);
+            const std::vector<unsigned char> tree = read_all(d + "panels/full_tree_" + its);
+            int64_t np = 0;
+            if (tree.size() < 8) fail(FS_ERR_ARG, "bad panel tree header for " + name);
+            std::memcpy(&np, tree.data(), 8);
+            const size_t rec = DiagOutput::kTreeRecord;
+            if (np <= 0 || tree.size() != 8 + rec * (size_t)np) fail(FS_ERR_ARG, "bad panel tree size for " + name);
+            HostMesh& M = meshes[k];
+            M = S.base_mesh.panels.empty() ? S.mesh : S.base_mesh;  // heights and bounds
+            M.panels.assign((size_t)np, HostPanel{});
+            const int npts = (int)hx[k].size();
+            for (int64_t i = 0; i < np; ++i) {
+                const unsigned char* r = tree.data() + 8 + rec * (size_t)i;
+                int32_t v[18];
+                std::memcpy(v, r, sizeof(v));
+                HostPanel& P = M.panels[(size_t)i];
+                std::memset(&P, 0, sizeof(P));
+                P.level = v[1];
+                P.parent = v[2];
+                P.which = v[3];
+                for (int q = 0; q < 9; ++q) {
+                    P.pts[q] = v[4 + q];
+                    if (P.pts[q] < 0 || P.pts[q] >= npts) fail(FS_ERR_ARG, "panel tree of " + name + " points outside its xs");
+                }
+                P.left = v[13];
+                P.top = v[14];
+                P.right = v[15];
+                P.bottom = v[16];
+                P.child = v[17];
+                const int8_t* b = reinterpret_cast<const int8_t*>(r + sizeof(v));
+                P.lb = b[0] != 0;
+                P.rb = b[1] != 0;
+                P.xp = b[2] != 0;
+                P.pr = b[3] != 0;
+                P.needs = b[4] != 0;
+                const int nc = P.xp ? 4 : (P.pr ? 2 : 0);
+                if (nc && (P.child <= (int)i || P.child + nc > np))
+                    fail(FS_ERR_ARG, "panel tree of " + name + " has children out of order");
+                // every index the device walks follow must name a panel: the
+                // point location reads the records of neighbours and parents
+                bool ok = P.parent >= -1 && P.parent < np && (i == 0) == (P.parent == -1);
+                for (int nb : {P.left, P.top, P.right, P.bottom}) ok = ok && nb >= -2 && nb < np && (nb != -1 || P.parent >= 0);
+                if (!ok) fail(FS_ERR_ARG, "panel tree of " + name + " has links outside the tree");
+            }
+            M.xs = hx[k];
+            M.ps = hp[k];
+            M.restart_leaves();
+            if (!S.adaptive && npts != S.nbase)
+                fail(FS_ERR_ARG, "restart files of " + name + " hold " + std::to_string(npts) +
+                                     " points; the deck's uniform mesh has " + std::to_string(S.nbase));
+            const std::vector<double> w = M.base_weights(S.q, prm.quadrature);
+            hq[k].resize(npts);
+            for (int i = 0; i < npts; ++i) hq[k][i] = w[i] * hf[k][i];
+        }
+        FS_CUDA(cudaStreamSynchronize(st));
+        for (int k = 0; k < ns; ++k) {
+            sp[k]->mesh = std::move(meshes[k]);
+            upload_mesh(*sp[k]);
+        }
+        relayout(hx, hp, hf, hq);
+        iter = it;
+        t = it * prm.dt;
+        remeshing = false;
+        reduced_field();
+        check_status();
+    }
+
     // A step (AMRSimulation::step, AMRSimulation_step.cpp:5-99) is four field
     // evaluations with work before and after each:
     //   0: RK stage 1 kernel, field at xk (epilogue: stage 2)
@@ -1417,6 +1522,18 @@ fs_status fs_sim_set_output(fs_sim* sim, const char* sim_dir, const char* const*
         for (int k = 0; k < S.prm.num_species; ++k)
             names.push_back(species_names && species_names[k] ? species_names[k] : "");
         S.set_output(sim_dir, names, diag_period, diag_phase_space_period);
+    });
+}
+
+fs_status fs_sim_restart(fs_sim* sim, const char* sim_dir, const char* const* species_names, int iter) {
+    return fsb::guard([&] {
+        if (!sim || !sim_dir) fsb::fail(FS_ERR_ARG, "null argument");
+        auto& S = sim->impl;
+        FS_CUDA(cudaSetDevice(S.prm.device));
+        std::vector<std::string> names;
+        for (int k = 0; k < S.prm.num_species; ++k)
+            names.push_back(species_names && species_names[k] ? species_names[k] : "");
+        S.restart(sim_dir, names, iter);
     });
 }
 

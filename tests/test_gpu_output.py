@@ -107,3 +107,57 @@ def test_dumps_follow_adaptive_meshes(tmp_path):
         inds = _read(out / "panels" / f"leaf_point_inds_{it}", np.int32)
         assert inds.max() == n - 1
     g.close()
+
+
+@pytest.mark.parametrize("adaptive", [False, True])
+def test_restart_from_dumps_continues_the_run(tmp_path, adaptive):
+    """Dump at iteration 4 (a remesh iteration), restart a fresh session from
+    the files: the loaded state equals the original, t = 4 dt, and three more
+    steps follow the original within rounding (the restart recomputes E on the
+    reduced grid).  Like the reference, the restart recomputes the weights from
+    the loaded leaves, which equals the carried weights when the dump was
+    taken right after a remesh."""
+    d = decks.two_stream(h=4, ph=1, steps=7, remesh_period=4)
+    if adaptive:
+        d["species_list"][0].update(do_adaptively_refine=True, max_height=6, amr_epsilons=[0.05])
+    g = M.Simulation(d, "direct64")
+    g.set_output(str(tmp_path), diag_period=2, diag_phase_space_period=2)
+    g.step(4)
+    g.flush_output()
+    ref4 = g.state()
+    r = M.Simulation(d, "direct64")
+    r.restart(str(tmp_path), 4)
+    it, t = r.iteration()
+    assert it == 4 and t == pytest.approx(4 * d["dt"], rel=1e-15)
+    got = r.state()
+    for k in ("xs", "ps", "fs", "q_ws"):
+        assert np.array_equal(got[k], ref4[k]), k
+    assert np.linalg.norm(got["es"] - ref4["es"]) <= 1e-12 * np.linalg.norm(ref4["es"])
+    g.step(3)
+    r.step(3)
+    a, b = r.state(), g.state()
+    assert len(a["xs"]) == len(b["xs"])
+    for k in ("xs", "ps", "fs", "es"):
+        assert np.linalg.norm(a[k] - b[k]) <= 1e-10 * np.linalg.norm(b[k]), k
+    g.close()
+    r.close()
+
+
+def test_restart_rejects_missing_or_corrupt_files(tmp_path):
+    d = decks.two_stream(h=4, ph=1, steps=2)
+    g = M.Simulation(d, "direct64")
+    with pytest.raises(M.FsError):
+        g.restart(str(tmp_path), 0)  # nothing written yet
+    g.set_output(str(tmp_path), 1, 1)
+    g.flush_output()
+    tree = tmp_path / "simulation_output" / "electrons" / "panels" / "full_tree_0"
+    raw = bytearray(tree.read_bytes())
+    raw[8 + 80 * 3 + 52:8 + 80 * 3 + 56] = np.int32(10 ** 6).tobytes()  # a neighbour far outside the tree
+    tree.write_bytes(bytes(raw))
+    before = g.state()
+    with pytest.raises(M.FsError):
+        g.restart(str(tmp_path), 0)
+    after = g.state()
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k  # the session is unchanged
+    g.close()
