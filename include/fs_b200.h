@@ -103,7 +103,11 @@ typedef struct fs_species_params {
     double q, m;
     int initial_height, p_height;
     double pmin, pmax;
-    int ics_type;                 /* 1,2 Landau; 3 strong two-stream; 4 colder two-stream; 9,10 ion acoustic */
+    int ics_type;                 /* 1,2 Landau; 3 strong two-stream; 4 colder two-stream;
+                                     5 Friedman beam; 6 Maxwell-Juttner; 7 relativistic
+                                     two-stream; 8 relativistic travelling wave; 9,10 ion
+                                     acoustic (make_f0_return_ptr,
+                                     AMRSimulation_load.cpp:139-225)                    */
     double pth, pstr, amp, normalized_wavenumber;
     /* Adaptive refinement (AMRSimulation_load.cpp:246-258; generate_mesh,
      * AMRStructure_amr.cpp:901-941): when on, panels of the uniform mesh whose
@@ -114,6 +118,11 @@ typedef struct fs_species_params {
     int max_height;
     int n_amr_eps;                /* 0..5; 0 turns the refinement off           */
     double amr_eps[5];
+    /* Deck keys of the relativistic initial conditions: "mu" (inverse
+     * temperature of ics 6 and 7; the reference's default 1.0 when the key is
+     * absent) and "wave_beta" (ics 8; default 0.8). */
+    double mu;
+    double wave_beta;
 } fs_species_params;
 
 /* Deck-level parameters (AMRSimulation_load.cpp:14-47). */
@@ -136,6 +145,13 @@ typedef struct fs_sim_params {
     int use_external_field;       /* 0 off                                      */
     int external_type;            /* 0 tanh, 1 sine, 2 logistic                 */
     double external_Am, external_k, external_omega;
+    /* Opt-in relativistic position push: every RK4 stage moves x with
+     * v = (p/m) / sqrt(1 + (p/m)^2) instead of p (the formula of
+     * AMRSimulation::relativistic_momentum_push, AMRSimulation_step.cpp:101-111).
+     * The reference defines that push but never calls it, and its
+     * "relativistic" deck key has no effect on rk4_step; 0 keeps that
+     * behaviour. */
+    int relativistic_push;
 } fs_sim_params;
 
 typedef struct fs_sim fs_sim;
@@ -167,6 +183,15 @@ fs_status fs_sim_pair_count(const fs_sim* sim, double* pairs);
  * (treecode: near pairs + far cluster terms; counted while profiling is
  * enabled, otherwise equal to the direct-equivalent count). */
 fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_evals);
+
+/* The initial distribution of species `species` of a deck at n phase-space
+ * points (distribution::operator() of the object make_f0_return_ptr builds,
+ * AMRSimulation_load.cpp:139-225, initial_distributions.cpp:11-460).  Host
+ * only: no device is touched.  Points where the reference would read past its
+ * tabulated Friedman-beam density or travelling-wave orbit are rejected with
+ * FS_ERR_ARG instead. */
+fs_status fs_initial_f0(const fs_sim_params* params, int species, int n, const double* x,
+                        const double* p, double* f);
 
 /* ------------------------------------------------------------------ batch */
 /* Many independent simulations stepped together on one device and stream

@@ -45,7 +45,7 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
            "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
            "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes", "fs_sim_set_output",
-           "fs_sim_flush_output", "fs_sim_restart"]
+           "fs_sim_flush_output", "fs_sim_restart", "fs_initial_f0"]
 
 
 class FsError(RuntimeError):
@@ -64,7 +64,7 @@ class SpeciesParams(C.Structure):
                 ("pmin", C.c_double), ("pmax", C.c_double), ("ics_type", C.c_int), ("pth", C.c_double),
                 ("pstr", C.c_double), ("amp", C.c_double), ("normalized_wavenumber", C.c_double),
                 ("do_adaptively_refine", C.c_int), ("max_height", C.c_int), ("n_amr_eps", C.c_int),
-                ("amr_eps", C.c_double * 5)]
+                ("amr_eps", C.c_double * 5), ("mu", C.c_double), ("wave_beta", C.c_double)]
 
 
 class SimParams(C.Structure):
@@ -73,7 +73,7 @@ class SimParams(C.Structure):
                 ("mac", C.c_double), ("degree", C.c_int), ("max_source", C.c_int), ("num_species", C.c_int),
                 ("species", SpeciesParams * 8), ("device", C.c_int), ("use_external_field", C.c_int),
                 ("external_type", C.c_int), ("external_Am", C.c_double), ("external_k", C.c_double),
-                ("external_omega", C.c_double)]
+                ("external_omega", C.c_double), ("relativistic_push", C.c_int)]
 
 
 class PoolParams(C.Structure):
@@ -133,6 +133,8 @@ def lib():
         L.fs_sim_restart.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_char_p), C.c_int]
         L.fs_sim_restart.restype = st
         L.fs_sim_flush_output.restype = st
+        L.fs_initial_f0.argtypes = [C.POINTER(SimParams), C.c_int, C.c_int, _dp, _dp, _dp]
+        L.fs_initial_f0.restype = st
         L.fs_profile_enable.argtypes = [C.c_int]
         L.fs_profile_read.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), _dp, _dp]
         L.fs_profile_reset.argtypes = []
@@ -342,7 +344,13 @@ def sim_params(deck: dict, field_backend: str | None = None, device: int = 0) ->
         S.n_amr_eps = len(eps)
         for k, e in enumerate(eps):
             S.amr_eps[k] = e
+        # relativistic initial conditions: the reference's defaults when the
+        # keys are absent (AMRSimulation_load.cpp:169-207)
+        S.mu, S.wave_beta = float(sp.get("mu", 1.0)), float(sp.get("wave_beta", 0.8))
     P.device = int(device)
+    # opt-in relativistic position push; the reference's own "relativistic"
+    # key has no effect on its RK4 step and is ignored here too
+    P.relativistic_push = 1 if int(deck.get("relativistic_push", 0)) > 0 else 0
     # "external_field" block (AMRSimulation_load.cpp:98-136); absent = off
     ext = deck.get("external_field") or {}
     if int(ext.get("use_external_field", 0)) > 0:
@@ -541,6 +549,20 @@ class Batch:
 
 
 # --------------------------------------------------------------------- serving
+def initial_f0(deck: dict, species: int, x, p) -> np.ndarray:
+    """f0 of species `species` of `deck` at the points (x, p): the
+    distribution make_f0_return_ptr builds (AMRSimulation_load.cpp:139-225).
+    Host code only; needs no device."""
+    P = sim_params(deck)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    if x.shape != p.shape:
+        raise FsError(1, "x and p differ in shape")
+    f = np.empty_like(x)
+    _check(lib().fs_initial_f0(C.byref(P), int(species), int(x.size), _ptr(x), _ptr(p), _ptr(f)))
+    return f
+
+
 def estimate_bytes(deck: dict, field_backend: str | None = None) -> float:
     """Device bytes a Pool reserves for this deck (host-only computation)."""
     p = sim_params(deck, field_backend)

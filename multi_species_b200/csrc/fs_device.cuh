@@ -25,6 +25,20 @@ __device__ __forceinline__ double stage_qm(const Stage& S, int o) {
     return qm;
 }
 
+// Position velocity of stage momentum p.  rk4_step moves x with p itself
+// (AMRSimulation_step.cpp:163, :184, :208, :245); with the opt-in relativistic
+// push it is relativistic_momentum_push's v = (p/m) / sqrt(1 + (p/m)^2)
+// (AMRSimulation_step.cpp:101-111), correctly rounded so it matches the host.
+__device__ __forceinline__ double stage_v(const Stage& S, int o, double p) {
+    if (!S.rel) return p;
+    double m = S.m[0];
+#pragma unroll
+    for (int s = 1; s < 8; ++s)
+        if (s < S.nsp && o >= S.start[s]) m = S.m[s];
+    const double u = __ddiv_rn(p, m);
+    return __ddiv_rn(u, __dsqrt_rn(dadd(1.0, dmul(u, u))));
+}
+
 // RK4 epilogue for point o given the raw field E at that point
 // (src/simulation_files/AMRSimulation_step.cpp:178-248).
 __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
@@ -38,8 +52,9 @@ __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
         case STAGE_RK2: {
             const double ef = dmul(E, stage_qm(S, o));
             const double p2 = S.pst[o];
-            S.xk[o] = dadd(S.x[o], dmul(S.hdt, p2));
-            S.accX[o] = dadd(S.accX[o], dmul(2.0, p2));
+            const double v2 = stage_v(S, o, p2);
+            S.xk[o] = dadd(S.x[o], dmul(S.hdt, v2));
+            S.accX[o] = dadd(S.accX[o], dmul(2.0, v2));
             S.accP[o] = dadd(S.accP[o], dmul(2.0, ef));
             S.pst[o] = dadd(S.p[o], dmul(S.hdt, ef));  // p3
             break;
@@ -47,8 +62,9 @@ __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
         case STAGE_RK3: {
             const double ef = dmul(E, stage_qm(S, o));
             const double p3 = S.pst[o];
-            S.xk[o] = dadd(S.x[o], dmul(S.dt, p3));
-            S.accX[o] = dadd(S.accX[o], dmul(2.0, p3));
+            const double v3 = stage_v(S, o, p3);
+            S.xk[o] = dadd(S.x[o], dmul(S.dt, v3));
+            S.accX[o] = dadd(S.accX[o], dmul(2.0, v3));
             S.accP[o] = dadd(S.accP[o], dmul(2.0, ef));
             S.pst[o] = dadd(S.p[o], dmul(S.dt, ef));  // p4
             break;
@@ -56,7 +72,7 @@ __device__ __forceinline__ void apply_stage(const Stage& S, int o, double E) {
         case STAGE_RK4: {
             const double ef = dmul(E, stage_qm(S, o));
             const double p4 = S.pst[o];
-            const double ax = dadd(S.accX[o], p4);
+            const double ax = dadd(S.accX[o], stage_v(S, o, p4));
             const double ap = dadd(S.accP[o], ef);
             S.x[o] = dadd(S.x[o], dmul(S.dt6, ax));
             S.p[o] = dadd(S.p[o], dmul(S.dt6, ap));

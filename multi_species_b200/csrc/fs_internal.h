@@ -128,6 +128,10 @@ struct Stage {
     int nsp = 1;
     int start[9] = {0};
     double qm[8] = {0};
+    // relativistic position push (rel != 0): stage positions move with
+    // v = (p/m) / sqrt(1 + (p/m)^2), m the species mass
+    int rel = 0;
+    double m[8] = {0};
     // drive field: E += ext_a * sin(ext_k * ext_x[o] - ext_omt) when ext_x is set
     // (ext_x = the evaluation's targets, in the caller's order)
     const double* ext_x = nullptr;
@@ -163,7 +167,19 @@ struct HostMesh {
     int np() const { return 2 * (1 << (h + ph)) + 1; }
 };
 
-double f0_value(int ics_type, double pth, double pstr, double k, double amp, double x, double p);
+// Initial distribution of one species (make_f0_return_ptr,
+// AMRSimulation_load.cpp:139-225): tables of the Friedman beam and the
+// relativistic wave are built once, K_1(mu) is evaluated once.
+struct InitialDistribution {
+    int ics;
+    double pth, pstr, amp, mu, wave_beta, k = 0;
+    double fb_xcf = 0, fb_nhat = 0, fb_pth = 0, fb_dx = 0;
+    std::vector<double> fb_N;          // Friedman envelope density, step 0.01
+    double k1mu = 0, gstr = 0;         // K_1(mu), sqrt(1 + pstr^2)
+    std::vector<double> wv_x, wv_p;    // cold travelling-wave orbit, 100 nodes
+    InitialDistribution(const fs_species_params& S, double xmin, double xmax);
+    double operator()(double x, double p) const;
+};
 
 // ------------------------------------------------------------------ field engines
 // Per sorted target of the FP32 direct sum (csrc/fs_direct32.cu).

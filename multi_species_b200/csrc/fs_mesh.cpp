@@ -466,29 +466,116 @@ void HostMesh::panel_records(int* out) const {
     }
 }
 
-// Initial distributions used by the decks (src/structure_files/initial_distributions.cpp:16-140).
-// Evaluated on the host with the C library's exp/cos so the initial state is
-// bit-identical to the reference's.
-double f0_value(int ics, double pth, double pstr, double k, double amp, double x, double p) {
+// Initial distributions (distribution::operator() of the objects built by
+// make_f0_return_ptr, AMRSimulation_load.cpp:139-225; initial_distributions.cpp).
+// Evaluated on the host in the reference's operation order with the C library's
+// exp/cos/sqrt, so the initial state is bit-identical to the reference's.  The
+// reference evaluates the modified Bessel function K_1 and the incomplete
+// elliptic integrals with Boost.Math; here they come from the C++17 standard
+// library (std::cyl_bessel_k, std::ellint_1, std::ellint_2).
+InitialDistribution::InitialDistribution(const fs_species_params& S, double xmin, double xmax)
+    : ics(S.ics_type), pth(S.pth), pstr(S.pstr), amp(S.amp), mu(S.mu), wave_beta(S.wave_beta) {
+    k = 2.0 * M_PI / (xmax - xmin) * S.normalized_wavenumber;
+    switch (ics) {
+        case 5: {  // F0_Friedman_beam(Delta = amp, Tstar = pth^2, xmax), :171-184, :241-262
+            const double k_beta_0 = 2.0 * M_PI / 3.0, lambda_D = 2.81e-4, beta_b = 2.343e-3;
+            const double gamma_b = 1.0 / std::sqrt(1 + beta_b * beta_b);
+            fb_xcf = 1.0 / k_beta_0 / lambda_D / gamma_b;
+            fb_nhat = 1.0 / (1.0 + amp);
+            fb_pth = std::sqrt(pth * pth);
+            const double dx = 0.01;
+            const double nxd = std::ceil(1.1 * (xmax * fb_xcf) / dx);
+            if (!(nxd >= 2) || nxd > 1e8) fail(FS_ERR_ARG, "Friedman beam: xmax gives no usable density table");
+            const int nx = (int)nxd;
+            fb_N.assign(nx, 0.0);
+            fb_N[0] = 1.0;
+            double Np = 0.0;  // dN/dx of the envelope equation, explicit Euler
+            for (int i = 1; i < nx; ++i) {
+                const double N0 = fb_N[i - 1];
+                if (N0 <= 1e-150) continue;  // FRIEDMAN_BEAM_MIN_N: density stays 0
+                fb_N[i] = N0 + dx * Np;
+                Np += dx * (N0 * N0 - N0 * (1 + amp) + 1.0 / N0 * Np * Np);
+            }
+            fb_dx = 1 * dx - 0.0;  // xs[1] - xs[0] of the reference's table
+            break;
+        }
+        case 6: case 7: {  // Maxwell_Jutner :306-313, Relativistic_Two_Stream :350-360
+            if (!(mu > 0)) fail(FS_ERR_ARG, "relativistic initial condition needs mu > 0");
+            k1mu = std::cyl_bessel_k(1.0, mu);
+            if (!(k1mu > 0) || !std::isfinite(k1mu)) fail(FS_ERR_ARG, "K_1(mu) is not representable for this mu");
+            gstr = std::sqrt(1 + pstr * pstr);
+            break;
+        }
+        case 8: {  // Relativistic_Wave(amp, wave_beta, pth): check_gamma, make_cold_xs_ps, :366-433
+            const double gm = amp;
+            if (!(gm >= 1)) fail(FS_ERR_ARG, "relativistic wave: amp (the maximum gamma) must be >= 1");
+            if (wave_beta < 1.0 && 1.0 / std::sqrt(1 - wave_beta * wave_beta) < gm)
+                fail(FS_ERR_ARG, "relativistic wave: particles faster than the wave (max gamma above the wave's)");
+            const double kap = std::sqrt((gm - 1.0) / (gm + 1.0));
+            const double kap_p = std::sqrt(2 / (gm + 1.0));
+            const int np = 100;
+            const double da = 3 * M_PI / (np - 1);
+            wv_x.resize(np);
+            wv_p.resize(np);
+            for (int i = 0; i < np; ++i) {
+                const double a = -M_PI / 2 + i * da;
+                const double x0 = wave_beta * (2 / kap_p * std::ellint_2(kap, a) - kap_p * std::ellint_1(kap, a));
+                wv_x[i] = x0 + 2 * kap / kap_p * std::sin(a);
+                const double g = gm - (gm - 1) * std::sin(a) * std::sin(a);
+                wv_p[i] = std::sqrt(g * g - 1) * (std::cos(a) > 0 ? 1 : -1);
+            }
+            break;
+        }
+        default:  // any other value: F0_LD, like the reference's default branch
+            break;
+    }
+}
+
+double InitialDistribution::operator()(double x, double p) const {
     const double c = 1.0 / std::sqrt(2.0 * M_PI);
     switch (ics) {
-        case 3: {  // p^2 * Landau seed with zero drift
+        case 3: {  // F0_strong_two_stream: p^2 times the Landau seed with zero drift
             double seed = c / pth * std::exp(-(p - 0.0) * (p - 0.0) / 2 / pth / pth) * (1 + amp * std::cos(k * x));
             return seed * p * p;
         }
-        case 4: {  // two drifting Maxwellians
+        case 4: {  // F0_colder_two_stream: two drifting Maxwellians
             double a = p - pstr, b = p + pstr;
             double ma = c / pth * std::exp(-(a - 0.0) * (a - 0.0) / 2 / pth / pth);
             double mb = c / pth * std::exp(-(b - 0.0) * (b - 0.0) / 2 / pth / pth);
             return .5 * (ma + mb) * (1 + amp * std::cos(k * x));
         }
-        case 1:
-        case 2:
-        case 9:
-        case 10:
+        case 5: {  // Maxwellian in 1.25 p times the tabulated envelope at |x| / 1.25
+            const double q = p * 1.25;
+            const double m = c / fb_pth * std::exp(-(q - 0.0) * (q - 0.0) / 2 / fb_pth / fb_pth);
+            const double u = std::fabs(x / 1.25) * fb_xcf / fb_dx;
+            const double fl = std::floor(u);
+            if (!(fl >= 0) || fl + 1 >= (double)fb_N.size())
+                fail(FS_ERR_ARG, "Friedman beam: x beyond the tabulated density (1.1 xmax)");
+            const int i = (int)fl;
+            const double th = u - fl;
+            return m * fb_nhat * ((1 - th) * fb_N[i] + th * fb_N[i + 1]);
+        }
+        case 6: {
+            const double g = std::sqrt(1 + p * p);
+            return std::exp(-g * mu) / 2.0 / k1mu * (1 + amp * std::cos(k * x));
+        }
+        case 7: {
+            const double g = std::sqrt(1 + p * p);
+            const double ppm = p * pstr * mu;
+            const double ep = std::exp(ppm - gstr * g * mu) / 2.0 / k1mu;
+            const double em = std::exp(-ppm - gstr * g * mu) / 2.0 / k1mu;
+            return (ep + em) / 2.0 * (1 + amp * std::cos(k * x));
+        }
+        case 8: {  // thermal spread around the cold orbit, linear in x between table nodes
+            if (!(x <= wv_x.back())) fail(FS_ERR_ARG, "relativistic wave: x beyond the tabulated orbit");
+            size_t i = 0;
+            while (x > wv_x[i + 1]) ++i;
+            const double th = x - wv_x[i];  // not normalised by the node spacing, as in the reference
+            const double p0 = (1 - th) * wv_p[i] + th * wv_p[i + 1];
+            return 1.0 / std::sqrt(2 * M_PI) / pth * std::exp(-(p - p0) * (p - p0) / 2 / pth / pth);
+        }
+        default:  // 1, 2, 9, 10 (and unknown values): F0_LD, F0_ion_acoustic_electron/_ion share this form
             return c / pth * std::exp(-(p - pstr) * (p - pstr) / 2 / pth / pth) * (1 + amp * std::cos(k * x));
-        default:
-            fail(FS_ERR_UNSUPPORTED, "ics_type " + std::to_string(ics) + " not supported");
     }
 }
 

@@ -61,16 +61,17 @@ constexpr int kHist = 1024;
 __device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
 
 // ---------------------------------------------------------------- RK4 stage 1
-// ef1 = E*qm, p2 = p + hdt*ef1, xk = x + hdt*p, accX = p, accP = ef1
-// (AMRSimulation_step.cpp:148-165).
+// ef1 = E*qm, p2 = p + hdt*ef1, xk = x + hdt*v(p), accX = v(p), accP = ef1
+// (AMRSimulation_step.cpp:148-165; v(p) = p unless the relativistic push is on).
 __global__ void k_rk_stage1(int n, Stage S, double* __restrict__ e, double* __restrict__ xk) {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= n) return;
     const double ef = dmul(e[o], stage_qm(S, o));
     const double p1 = S.p[o];
+    const double v1 = stage_v(S, o, p1);
     S.pst[o] = dadd(p1, dmul(S.hdt, ef));
-    xk[o] = dadd(S.x[o], dmul(S.hdt, p1));
-    S.accX[o] = p1;
+    xk[o] = dadd(S.x[o], dmul(S.hdt, v1));
+    S.accX[o] = v1;
     S.accP[o] = ef;
 }
 
@@ -929,11 +930,10 @@ struct Sim {
             ss->mesh.build(S.initial_height, S.p_height, P.xmin, P.xmax, S.pmin, S.pmax);
             HostMesh& M = ss->mesh;
             ss->nbase = (int)M.xs.size();
-            const double kx = 2.0 * M_PI / L * S.normalized_wavenumber;
             // initial condition (AMRStructure ctor / generate_mesh at the initial step)
+            const InitialDistribution dist(S, P.xmin, P.xmax);
             std::vector<double> f0(M.xs.size());
-            for (size_t i = 0; i < f0.size(); ++i)
-                f0[i] = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, M.xs[i], M.ps[i]);
+            for (size_t i = 0; i < f0.size(); ++i) f0[i] = dist(M.xs[i], M.ps[i]);
             ss->adaptive = S.do_adaptively_refine && S.n_amr_eps > 0;
             if (ss->adaptive) {
                 if (S.n_amr_eps > 5) fail(FS_ERR_ARG, "at most 5 amr_epsilons");
@@ -943,7 +943,7 @@ struct Sim {
                 ss->base_mesh = M;
                 M.adapt(f0, ss->eps, ss->neps, ss->max_height,
                         [&](const double* x, const double* p, int n, double* out) {
-                            for (int i = 0; i < n; ++i) out[i] = f0_value(S.ics_type, S.pth, S.pstr, kx, S.amp, x[i], p[i]);
+                            for (int i = 0; i < n; ++i) out[i] = dist(x[i], p[i]);
                         });
             }
             ss->start = N;
@@ -956,6 +956,7 @@ struct Sim {
             ss->nleaves = (int)M.leaves.size();
             base.start[s] = N;
             base.qm[s] = ss->qm;
+            base.m[s] = ss->m;
             N += ss->n;
             // weights (set_leaves_weights)
             std::vector<double> w0 = M.base_weights(S.q, P.quadrature);
@@ -1007,6 +1008,7 @@ struct Sim {
         }
         base.start[P.num_species] = N;
         for (int s = P.num_species + 1; s < 9; ++s) base.start[s] = N;
+        base.rel = P.relativistic_push ? 1 : 0;
         base.dt = P.dt;
         base.hdt = 0.5 * P.dt;
         base.dt6 = P.dt / 6.0;
@@ -1611,6 +1613,17 @@ fs_status fs_sim_work(const fs_sim* sim, double* direct_pairs, double* kernel_ev
         if (!sim) fsb::fail(FS_ERR_ARG, "null argument");
         if (direct_pairs) *direct_pairs = sim->impl.pairs;
         if (kernel_evals) *kernel_evals = sim->impl.evals;
+    });
+}
+
+fs_status fs_initial_f0(const fs_sim_params* params, int species, int n, const double* x,
+                        const double* p, double* f) {
+    return fsb::guard([&] {
+        if (!params || n < 0 || (n > 0 && (!x || !p || !f))) fsb::fail(FS_ERR_ARG, "null argument");
+        if (species < 0 || species >= params->num_species || species >= 8) fsb::fail(FS_ERR_ARG, "species out of range");
+        if (!(params->xmax > params->xmin)) fsb::fail(FS_ERR_ARG, "xmax must exceed xmin");
+        const fsb::InitialDistribution dist(params->species[species], params->xmin, params->xmax);
+        for (int i = 0; i < n; ++i) f[i] = dist(x[i], p[i]);
     });
 }
 

@@ -45,6 +45,19 @@ def bump_on_tail(h=9, ph=1, steps=50, amp=0.04):
                               dict(sp, name="ions", ics_type=9, pth=ION_PTH, pstr=0.0, amp=0.0, q=1.0, m=1836.0)])
 
 
+def relativistic_two_stream(h=5, ph=1, steps=20, mu=25.0, pstr=1.0, amp=0.01, push=True, remesh_period=5):
+    """Relativistic two-stream (ics 7: two boosted Maxwell-Juttner beams at
+    +-pstr with inverse temperature mu) on [0, 4 pi), p in [-4, 4], eps 0.05,
+    dt 0.2, electrons only; positions move with the relativistic velocity
+    p / sqrt(1 + p^2) when `push` is set."""
+    L = 4 * math.pi
+    return dict(xmin=0.0, xmax=L, pmin=-4.0, pmax=4.0, bcs=0, greens_epsilon=0.05, dt=0.2, num_steps=steps,
+                remesh_period=remesh_period, use_treecode=0, quadrature=0, relativistic_push=1 if push else 0,
+                species_list=[dict(name="electrons", ics_type=7, mu=mu, pstr=pstr, amp=amp,
+                                   normalized_wavenumber=1.0, q=-1.0, m=1.0, initial_height=h, p_height=ph,
+                                   pmin=-4.0, pmax=4.0)])
+
+
 def _quantized_mesh(target_per_species, nsp, lo=2000, hi=200000):
     """(h, ph) with h in 4..8, ph in 0..2 whose point count (2*2^h+1)*(2*2^(h+ph)+1)
     is closest in log to the per-species target, with the instance total in

@@ -45,7 +45,7 @@ class FsoSpecies(C.Structure):
                 ("ics_type", C.c_int), ("pth", C.c_double), ("pstr", C.c_double),
                 ("amp", C.c_double), ("normalized_wavenumber", C.c_double),
                 ("do_adaptively_refine", C.c_int), ("max_height", C.c_int), ("n_amr_eps", C.c_int),
-                ("amr_eps", C.c_double * 5)]
+                ("amr_eps", C.c_double * 5), ("mu", C.c_double), ("wave_beta", C.c_double)]
 
 
 class FsoSim(C.Structure):
@@ -54,7 +54,7 @@ class FsoSim(C.Structure):
                 ("use_treecode", C.c_int), ("mac", C.c_double), ("degree", C.c_int),
                 ("max_source", C.c_int), ("num_species", C.c_int), ("species", FsoSpecies * 8),
                 ("use_external_field", C.c_int), ("external_type", C.c_int), ("ext_Am", C.c_double),
-                ("ext_k", C.c_double), ("ext_omega", C.c_double)]
+                ("ext_k", C.c_double), ("ext_omega", C.c_double), ("relativistic_push", C.c_int)]
 
 
 _lib = None
@@ -82,6 +82,17 @@ def lib():
         L.fso_mesh_base_weights.argtypes = [C.c_void_p, C.c_double, C.c_int, _dp]
         L.fso_f0.argtypes = [C.c_int] + [C.c_double] * 6
         L.fso_f0.restype = C.c_double
+        L.fso_dist_create.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_int)]
+        L.fso_dist_create.restype = C.c_void_p
+        L.fso_dist_eval.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_int)]
+        L.fso_dist_eval.restype = C.c_double
+        L.fso_dist_destroy.argtypes = [C.c_void_p]
+        for n in ("fso_bessel_k1",):
+            getattr(L, n).argtypes = [C.c_double]
+            getattr(L, n).restype = C.c_double
+        for n in ("fso_ellint_1", "fso_ellint_2"):
+            getattr(L, n).argtypes = [C.c_double, C.c_double]
+            getattr(L, n).restype = C.c_double
         L.fso_remesh_interp.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, _dp, _ip, _dp]
         L.fso_remesh_interp.restype = C.c_int
         L.fso_reduce.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _ip]
@@ -293,6 +304,39 @@ def f0(ics, pth, pstr, k, amp, x, p):
     return np.array([fn(ics, pth, pstr, k, amp, float(a), float(b)) for a, b in zip(x, p)])
 
 
+def initial_f0(deck: dict, species: int, x, p):
+    """f0 of one species of a deck at the points (x, p): the distribution
+    make_f0_return_ptr builds (AMRSimulation_load.cpp:139-225), every ics_type.
+    Raises ValueError for invalid parameters or points beyond the
+    Friedman-beam / travelling-wave tables."""
+    P = sim_params(deck)
+    rc = C.c_int(0)
+    d = lib().fso_dist_create(C.byref(P.species[species]), P.xmin, P.xmax, C.byref(rc))
+    if not d:
+        raise ValueError("invalid initial-condition parameters")
+    try:
+        out = np.empty(len(x))
+        for i, (a, b) in enumerate(zip(np.asarray(x, dtype=np.float64), np.asarray(p, dtype=np.float64))):
+            out[i] = lib().fso_dist_eval(d, float(a), float(b), C.byref(rc))
+        if rc.value:
+            raise ValueError("point beyond the tabulated initial condition")
+        return out
+    finally:
+        lib().fso_dist_destroy(d)
+
+
+def bessel_k1(x):
+    return lib().fso_bessel_k1(float(x))
+
+
+def ellint_1(k, phi):
+    return lib().fso_ellint_1(float(k), float(phi))
+
+
+def ellint_2(k, phi):
+    return lib().fso_ellint_2(float(k), float(phi))
+
+
 def reduce(xs, q):
     xs, q = _f64(xs), _f64(q)
     n = len(xs)
@@ -337,6 +381,8 @@ def sim_params(deck: dict) -> FsoSim:
         S.do_adaptively_refine, S.max_height, S.n_amr_eps = amr[0], amr[1], len(amr[2])
         for k, e in enumerate(amr[2]):
             S.amr_eps[k] = e
+        S.mu, S.wave_beta = float(sp.get("mu", 1.0)), float(sp.get("wave_beta", 0.8))
+    P.relativistic_push = 1 if int(deck.get("relativistic_push", 0)) > 0 else 0
     ext = deck.get("external_field") or {}
     P.use_external_field = 1 if int(ext.get("use_external_field", 0)) > 0 else 0
     if P.use_external_field:

@@ -604,6 +604,200 @@ double fso_f0(int ics, double pth, double pstr, double k, double amp, double x, 
     }
 }
 
+/* ---- special functions of the relativistic initial conditions ---- */
+double fso_bessel_k1(double x) {
+    /* K_1(x) = exp(-x) int_0^inf exp(-x (cosh t - 1)) cosh t dt.  The integrand
+     * is even in t and analytic in |Im t| < pi/2, so the trapezoid rule on the
+     * half line converges like exp(-pi^2 / h); for large x the integrand is a
+     * Gaussian of width 1/sqrt(x), whose error exp(-2 pi^2 / (h^2 x)) sets
+     * h <= 0.25 / sqrt(x).  cosh t - 1 = 2 sinh^2(t/2) keeps the exponent
+     * accurate near t = 0; the terms are added with Neumaier's compensated sum. */
+    if (!(x > 0)) return NAN;
+    const double h = fmin(1.0 / 16, 0.25 / sqrt(x));
+    double sum = 0.5, comp = 0.0;
+    for (int i = 1; i < 10000000; ++i) {
+        const double t = i * h, sh = sinh(0.5 * t), ch = cosh(t);
+        const double term = exp(-x * (2.0 * sh * sh)) * ch;
+        const double y = sum + term;
+        comp += fabs(sum) >= fabs(term) ? (sum - y) + term : (term - y) + sum;
+        sum = y;
+        if (term < 1e-20 * sum) break;
+    }
+    return exp(-x) * ((sum + comp) * h);
+}
+
+/* Carlson's R_F(x, y, z) and R_D(x, y, z): duplicate until every relative
+ * deviation from the mean is below 2e-5, then the fifth-order series. */
+static double carlson_rf(double x, double y, double z) {
+    for (int it = 0; it < 200; ++it) {
+        const double A = (x + y + z) / 3.0;
+        const double X = 1.0 - x / A, Y = 1.0 - y / A, Z = 1.0 - z / A;
+        if (fmax(fabs(X), fmax(fabs(Y), fabs(Z))) < 2e-5) {
+            const double e2 = X * Y - Z * Z, e3 = X * Y * Z;
+            return (1.0 - e2 / 10.0 + e3 / 14.0 + e2 * e2 / 24.0 - 3.0 * e2 * e3 / 44.0) / sqrt(A);
+        }
+        const double sx = sqrt(x), sy = sqrt(y), sz = sqrt(z);
+        const double lam = sx * sy + sy * sz + sz * sx;
+        x = 0.25 * (x + lam);
+        y = 0.25 * (y + lam);
+        z = 0.25 * (z + lam);
+    }
+    return NAN;
+}
+static double carlson_rd(double x, double y, double z) {
+    double sum = 0.0, fac = 1.0;
+    for (int it = 0; it < 200; ++it) {
+        const double A = (x + y + 3.0 * z) / 5.0;
+        const double X = 1.0 - x / A, Y = 1.0 - y / A, Z = 1.0 - z / A;
+        if (fmax(fabs(X), fmax(fabs(Y), fabs(Z))) < 2e-5) {
+            const double xy = X * Y, zz = Z * Z;
+            const double e2 = xy - 6.0 * zz, e3 = (3.0 * xy - 8.0 * zz) * Z;
+            const double e4 = 3.0 * (xy - zz) * zz, e5 = xy * zz * Z;
+            const double ser = 1.0 - 3.0 * e2 / 14.0 + e3 / 6.0 + 9.0 * e2 * e2 / 88.0 - 3.0 * e4 / 22.0
+                             - 9.0 * e2 * e3 / 52.0 + 3.0 * e5 / 26.0;
+            return 3.0 * sum + fac * ser / (A * sqrt(A));
+        }
+        const double sx = sqrt(x), sy = sqrt(y), sz = sqrt(z);
+        const double lam = sx * sy + sy * sz + sz * sx;
+        sum += fac / (sz * (z + lam));
+        fac *= 0.25;
+        x = 0.25 * (x + lam);
+        y = 0.25 * (y + lam);
+        z = 0.25 * (z + lam);
+    }
+    return NAN;
+}
+/* phi reduced to [-pi/2, pi/2] plus n half periods */
+static double ell_reduce(double phi, double* n) {
+    *n = floor(phi / M_PI + 0.5);
+    return phi - *n * M_PI;
+}
+double fso_ellint_1(double k, double phi) {
+    double n;
+    const double r = ell_reduce(phi, &n), s = sin(r), c = cos(r);
+    double v = s * carlson_rf(c * c, 1.0 - k * k * s * s, 1.0);
+    if (n != 0) v += 2.0 * n * carlson_rf(0.0, 1.0 - k * k, 1.0);
+    return v;
+}
+double fso_ellint_2(double k, double phi) {
+    double n;
+    const double r = ell_reduce(phi, &n), s = sin(r), c = cos(r), kk = k * k, y = 1.0 - kk * s * s;
+    double v = s * carlson_rf(c * c, y, 1.0) - kk * s * s * s * carlson_rd(c * c, y, 1.0) / 3.0;
+    if (n != 0)
+        v += 2.0 * n * (carlson_rf(0.0, 1.0 - kk, 1.0) - kk * carlson_rd(0.0, 1.0 - kk, 1.0) / 3.0);
+    return v;
+}
+
+/* ---- make_f0_return_ptr (AMRSimulation_load.cpp:139-225) ---- */
+#define FSO_WAVE_NODES 100
+struct fso_dist {
+    int ics;
+    double pth, pstr, amp, k, mu;
+    /* F0_Friedman_beam (initial_distributions.cpp:171-184, 241-290) */
+    double fb_xcf, fb_nhat, fb_pth, fb_dx;
+    int fb_n;
+    double* fb_N;
+    /* Maxwell_Jutner / Relativistic_Two_Stream (:306-313, :350-360) */
+    double k1mu, gstr;
+    /* Relativistic_Wave (:366-452) */
+    double wv_x[FSO_WAVE_NODES], wv_p[FSO_WAVE_NODES];
+};
+
+fso_dist* fso_dist_create(const fso_species_params* q, double xmin, double xmax, int* rc) {
+    *rc = 0;
+    fso_dist* d = (fso_dist*)calloc(1, sizeof(fso_dist));
+    d->ics = q->ics_type;
+    d->pth = q->pth; d->pstr = q->pstr; d->amp = q->amp; d->mu = q->mu;
+    d->k = 2.0 * M_PI / (xmax - xmin) * q->normalized_wavenumber;  /* kx of make_f0_return_ptr */
+    if (d->ics == 5) {
+        /* Delta = amp, Tstar = pth^2, xmax = the deck's xmax; the envelope
+         * N'' = N^2 - (1 + Delta) N + N'^2 / N, N(0) = 1, N'(0) = 0, by explicit
+         * Euler with step 0.01 out to 1.1 xmax in units of gamma_b lambda_D */
+        const double kb0 = 2.0 * M_PI / 3.0, lamD = 2.81e-4, bb = 2.343e-3;
+        const double gb = 1.0 / sqrt(1 + bb * bb);
+        const double dx = 0.01;
+        d->fb_xcf = 1.0 / kb0 / lamD / gb;
+        d->fb_nhat = 1.0 / (1.0 + d->amp);
+        d->fb_pth = sqrt(q->pth * q->pth);
+        const double nxd = ceil(1.1 * (xmax * d->fb_xcf) / dx);
+        if (!(nxd >= 2) || nxd > 1e8) { *rc = 1; fso_dist_destroy(d); return NULL; }
+        d->fb_n = (int)nxd;
+        d->fb_N = (double*)calloc((size_t)d->fb_n, sizeof(double));
+        d->fb_N[0] = 1.0;
+        double dN = 0.0;
+        for (int i = 1; i < d->fb_n; ++i) {
+            const double n0 = d->fb_N[i - 1];
+            if (n0 <= 1e-150) continue;  /* density below the floor stays 0 */
+            d->fb_N[i] = n0 + dx * dN;
+            dN += dx * (n0 * n0 - n0 * (1 + d->amp) + 1.0 / n0 * dN * dN);
+        }
+        d->fb_dx = 1 * dx - 0.0;
+    } else if (d->ics == 6 || d->ics == 7) {
+        if (!(d->mu > 0)) { *rc = 1; fso_dist_destroy(d); return NULL; }
+        d->k1mu = fso_bessel_k1(d->mu);
+        if (!(d->k1mu > 0) || !isfinite(d->k1mu)) { *rc = 1; fso_dist_destroy(d); return NULL; }
+        d->gstr = sqrt(1 + d->pstr * d->pstr);
+    } else if (d->ics == 8) {
+        /* cold orbit of a wave with maximum gamma gm = amp and phase velocity
+         * wave_beta, sampled at 100 values of the orbit parameter alpha in
+         * [-pi/2, 5 pi/2] */
+        const double gm = d->amp, wb = q->wave_beta;
+        if (!(gm >= 1) || (wb < 1.0 && 1.0 / sqrt(1 - wb * wb) < gm)) { *rc = 1; fso_dist_destroy(d); return NULL; }
+        const double kap = sqrt((gm - 1.0) / (gm + 1.0)), kp = sqrt(2 / (gm + 1.0));
+        const double da = 3 * M_PI / (FSO_WAVE_NODES - 1);
+        for (int i = 0; i < FSO_WAVE_NODES; ++i) {
+            const double a = -M_PI / 2 + i * da;
+            const double x0 = wb * (2 / kp * fso_ellint_2(kap, a) - kp * fso_ellint_1(kap, a));
+            d->wv_x[i] = x0 + 2 * kap / kp * sin(a);
+            const double g = gm - (gm - 1) * sin(a) * sin(a);
+            d->wv_p[i] = sqrt(g * g - 1) * (cos(a) > 0 ? 1 : -1);
+        }
+    }
+    return d;
+}
+
+double fso_dist_eval(const fso_dist* d, double x, double p, int* rc) {
+    const double c = 1.0 / sqrt(2.0 * M_PI);
+    switch (d->ics) {
+    case 5: {
+        const double pp = p * 1.25;  /* maxwellian(x, p mu) nhat N(x / mu), mu = 1.25 */
+        const double m = c / d->fb_pth * exp(-(pp - 0.0) * (pp - 0.0) / 2 / d->fb_pth / d->fb_pth);
+        const double u = fabs(x / 1.25) * d->fb_xcf / d->fb_dx;
+        const double fl = floor(u);
+        if (!(fl >= 0) || fl + 1 >= (double)d->fb_n) { *rc = 1; return 0.0; }
+        const int i = (int)fl;
+        const double th = u - fl;
+        return m * d->fb_nhat * ((1 - th) * d->fb_N[i] + th * d->fb_N[i + 1]);
+    }
+    case 6: {
+        const double g = sqrt(1 + p * p);
+        return exp(-g * d->mu) / 2.0 / d->k1mu * (1 + d->amp * cos(d->k * x));
+    }
+    case 7: {
+        const double g = sqrt(1 + p * p), ppm = p * d->pstr * d->mu;
+        const double ep = exp(ppm - d->gstr * g * d->mu) / 2.0 / d->k1mu;
+        const double em = exp(-ppm - d->gstr * g * d->mu) / 2.0 / d->k1mu;
+        return (ep + em) / 2.0 * (1 + d->amp * cos(d->k * x));
+    }
+    case 8: {
+        if (!(x <= d->wv_x[FSO_WAVE_NODES - 1])) { *rc = 1; return 0.0; }
+        int i = 0;
+        while (x > d->wv_x[i + 1]) ++i;
+        const double th = x - d->wv_x[i];  /* offset from the node, not normalised */
+        const double p0 = (1 - th) * d->wv_p[i] + th * d->wv_p[i + 1];
+        return 1.0 / sqrt(2 * M_PI) / d->pth * exp(-(p - p0) * (p - p0) / 2 / d->pth / d->pth);
+    }
+    default:
+        return fso_f0(d->ics, d->pth, d->pstr, d->k, d->amp, x, p);
+    }
+}
+
+void fso_dist_destroy(fso_dist* d) {
+    if (!d) return;
+    free(d->fb_N);
+    free(d);
+}
+
 /* ======================================================================= */
 /* Remesh: point location and 9-point fit                                   */
 /* ======================================================================= */
@@ -1149,10 +1343,14 @@ static void sim_reduced_field(fso_sim* s) {
     free(rx); free(rw); free(inv); free(re);
 }
 
-typedef struct { const fso_species_params* q; double kx; } f0_ctx;
+typedef struct { const fso_dist* d; int rc; } f0_ctx;
 static void eval_f0(void* ctx, const double* x, const double* p, int n, double* out) {
-    const f0_ctx* c = (const f0_ctx*)ctx;
-    for (int i = 0; i < n; ++i) out[i] = fso_f0(c->q->ics_type, c->q->pth, c->q->pstr, c->kx, c->q->amp, x[i], p[i]);
+    f0_ctx* c = (f0_ctx*)ctx;
+    for (int i = 0; i < n; ++i) {
+        int rc = 0;
+        out[i] = fso_dist_eval(c->d, x[i], p[i], &rc);
+        if (rc) c->rc = rc;
+    }
 }
 typedef struct {
     const fso_mesh* old_m;
@@ -1180,14 +1378,20 @@ fso_sim* fso_sim_create(const fso_sim_params* prm) {
         const fso_species_params* q = &prm->species[sp];
         s->mesh[sp] = fso_mesh_build(q->initial_height, q->p_height, prm->xmin, prm->xmax, q->pmin, q->pmax);
         if (!s->mesh[sp]) { fso_sim_destroy(s); return NULL; }
-        if (q->do_adaptively_refine && q->n_amr_eps > 0) {
-            /* generate_mesh at the initial step: f0 at every point, new ones included */
-            fso_mesh* m = s->mesh[sp];
-            f0_ctx fc = {q, 2.0 * M_PI / s->Lx * q->normalized_wavenumber};
-            double* f = (double*)malloc(sizeof(double) * m->npts);
-            eval_f0(&fc, m->xs, m->ps, m->npts, f);
-            f_init[sp] = fso_mesh_adapt(m, f, q->amr_eps, q->n_amr_eps, q->max_height, eval_f0, &fc);
-        }
+        /* the initial condition (AMRStructure ctor / generate_mesh at the initial step) */
+        int drc = 0;
+        fso_dist* dist = fso_dist_create(q, prm->xmin, prm->xmax, &drc);
+        if (!dist) { fso_sim_destroy(s); return NULL; }
+        fso_mesh* m = s->mesh[sp];
+        f0_ctx fc = {dist, 0};
+        double* f = (double*)malloc(sizeof(double) * m->npts);
+        eval_f0(&fc, m->xs, m->ps, m->npts, f);
+        /* fso_mesh_adapt reallocates f and returns it */
+        f_init[sp] = (q->do_adaptively_refine && q->n_amr_eps > 0)
+                         ? fso_mesh_adapt(m, f, q->amr_eps, q->n_amr_eps, q->max_height, eval_f0, &fc)
+                         : f;
+        fso_dist_destroy(dist);
+        if (fc.rc) { for (int k = 0; k <= sp; ++k) free(f_init[k]); fso_sim_destroy(s); return NULL; }
         s->start[sp] = tot;
         tot += s->mesh[sp]->npts;
     }
@@ -1202,8 +1406,6 @@ fso_sim* fso_sim_create(const fso_sim_params* prm) {
         const fso_species_params* q = &prm->species[sp];
         const fso_mesh* m = s->mesh[sp];
         const int a = s->start[sp];
-        /* make_f0_return_ptr: kx = 2 pi / Lx * normalized_wavenumber */
-        const double kx = 2.0 * M_PI / s->Lx * q->normalized_wavenumber;
         s->qm[sp] = q->q / q->m;
         s->w0[sp] = (double*)malloc(sizeof(double) * m->npts);
         fso_mesh_base_weights(m, q->q, prm->quadrature, s->w0[sp]);
@@ -1211,8 +1413,7 @@ fso_sim* fso_sim_create(const fso_sim_params* prm) {
         for (int i = 0; i < m->npts; ++i) {
             s->xs[a + i] = m->xs[i];
             s->ps[a + i] = m->ps[i];
-            s->fs[a + i] = f_init[sp] ? f_init[sp][i]
-                                      : fso_f0(q->ics_type, q->pth, q->pstr, kx, q->amp, m->xs[i], m->ps[i]);
+            s->fs[a + i] = f_init[sp][i];
             s->qws[a + i] = s->w0[sp][i] * s->fs[a + i];
             if (i == 0 || s->fs[a + i] < fmin) fmin = s->fs[a + i];
         }
@@ -1230,6 +1431,18 @@ void fso_sim_destroy(fso_sim* s) {
     free(s);
 }
 
+/* relativistic_momentum_push's velocity (AMRSimulation_step.cpp:101-111):
+ * v = (p/m) / sqrt(1 + (p/m)^2) with the species mass m */
+static void push_velocity(const fso_sim* s, const double* p, double* v) {
+    for (int sp = 0; sp < s->prm.num_species; ++sp) {
+        const double m = s->prm.species[sp].m;
+        for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
+            const double u = p[i] / m;
+            v[i] = u / sqrt(1 + u * u);
+        }
+    }
+}
+
 /* AMRSimulation::rk4_step (src/simulation_files/AMRSimulation_step.cpp:122-263). */
 static void sim_rk4(fso_sim* s) {
     const int N = s->N, ns = s->prm.num_species;
@@ -1245,35 +1458,49 @@ static void sim_rk4(fso_sim* s) {
     double* e4 = (double*)malloc(sizeof(double) * N);
     memcpy(p1, s->ps, sizeof(double) * N);
     memcpy(e1, s->es, sizeof(double) * N);
+    /* v1..v4: the stage momenta, or with the relativistic push their velocities */
+    double* v1 = p1; double* v2 = p2; double* v3 = p3; double* v4 = p4;
+    const int rel = s->prm.relativistic_push != 0;
+    if (rel) {
+        v1 = (double*)malloc(sizeof(double) * N);
+        v2 = (double*)malloc(sizeof(double) * N);
+        v3 = (double*)malloc(sizeof(double) * N);
+        v4 = (double*)malloc(sizeof(double) * N);
+        push_velocity(s, p1, v1);
+    }
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
             e1[i] *= s->qm[sp];
             p2[i] = s->ps[i] + 0.5 * dt * e1[i];
-            xk[i] = s->xs[i] + 0.5 * dt * p1[i];
+            xk[i] = s->xs[i] + 0.5 * dt * v1[i];
         }
+    if (rel) push_velocity(s, p2, v2);
     const double t2 = s->t + dt * 0.5, t4 = s->t + dt;  /* rk4_step :170, :201, :224 */
     sim_field(s, e2, xk, s->qws, N, t2);
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
             e2[i] *= s->qm[sp];
             p3[i] = s->ps[i] + 0.5 * dt * e2[i];
-            xk[i] = s->xs[i] + 0.5 * dt * p2[i];
+            xk[i] = s->xs[i] + 0.5 * dt * v2[i];
         }
+    if (rel) push_velocity(s, p3, v3);
     sim_field(s, e3, xk, s->qws, N, t2);
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) {
             e3[i] *= s->qm[sp];
             p4[i] = s->ps[i] + dt * e3[i];
-            xk[i] = s->xs[i] + dt * p3[i];
+            xk[i] = s->xs[i] + dt * v3[i];
         }
+    if (rel) push_velocity(s, p4, v4);
     sim_field(s, e4, xk, s->qws, N, t4);
     s->full_evals += 3;
     for (int sp = 0; sp < ns; ++sp)
         for (int i = s->start[sp]; i < s->start[sp + 1]; ++i) e4[i] *= s->qm[sp];
     for (int i = 0; i < N; ++i) {
-        s->xs[i] += dt / 6.0 * (p1[i] + 2 * p2[i] + 2 * p3[i] + p4[i]);
+        s->xs[i] += dt / 6.0 * (v1[i] + 2 * v2[i] + 2 * v3[i] + v4[i]);
         s->ps[i] += dt / 6.0 * (e1[i] + 2 * e2[i] + 2 * e3[i] + e4[i]);
     }
+    if (rel) { free(v1); free(v2); free(v3); free(v4); }
     free(xk); free(p1); free(p2); free(p3); free(p4); free(e1); free(e2); free(e3); free(e4);
 }
 

@@ -121,7 +121,27 @@ typedef struct {
     int max_height;
     int n_amr_eps;              /* 0..5 */
     double amr_eps[5];
+    /* "mu" of ics 6 and 7, "wave_beta" of ics 8 (AMRSimulation_load.cpp:169-207) */
+    double mu, wave_beta;
 } fso_species_params;
+
+/* The distribution make_f0_return_ptr builds (AMRSimulation_load.cpp:139-225)
+ * for every ics_type, with the Friedman-beam and travelling-wave tables.
+ * fso_dist_create returns NULL and sets *rc when the parameters are invalid
+ * (rc 1: argument; the reference throws or reads out of range there);
+ * fso_dist_eval sets *rc = 1 where the reference would read past a table. */
+typedef struct fso_dist fso_dist;
+fso_dist* fso_dist_create(const fso_species_params* q, double xmin, double xmax, int* rc);
+double fso_dist_eval(const fso_dist* d, double x, double p, int* rc);
+void fso_dist_destroy(fso_dist* d);
+/* Special functions of the relativistic initial conditions, restated from
+ * their definitions: K_1 by the trapezoid rule on
+ * int_0^inf exp(-x cosh t) cosh t dt, F and E by Carlson's symmetric
+ * integrals R_F and R_D with the duplication theorem (B. C. Carlson, Numer.
+ * Algorithms 10 (1995) 13-26) and F(k, phi + n pi) = F(k, phi) + 2 n K(k). */
+double fso_bessel_k1(double x);
+double fso_ellint_1(double k, double phi);
+double fso_ellint_2(double k, double phi);
 
 typedef struct {
     double xmin, xmax;
@@ -139,6 +159,10 @@ typedef struct {
     int use_external_field;
     int external_type;   /* 0 tanh, 1 sine, 2 logistic */
     double ext_Am, ext_k, ext_omega;
+    /* positions move with (p/m)/sqrt(1 + (p/m)^2) in every RK4 stage
+     * (relativistic_momentum_push, AMRSimulation_step.cpp:101-111); 0 = the
+     * reference's rk4_step, which moves them with p */
+    int relativistic_push;
 } fso_sim_params;
 
 typedef struct fso_sim fso_sim;

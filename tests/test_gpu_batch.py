@@ -193,3 +193,30 @@ def test_adaptive_member_alone_and_in_batch_bit_identical():
         assert np.array_equal(alone[k], mixed[k]), k
     b1.close()
     b2.close()
+
+
+def test_relativistic_member_alone_and_in_batch_bit_identical():
+    """A member with the relativistic push (positions move with p/sqrt(1+p^2))
+    steps in a batch, graph-captured, exactly as alone; its push does not leak
+    into the other members."""
+    rd = decks.relativistic_two_stream(h=4, ph=1, steps=7)
+    others = _small_decks(2, seed=59)
+    b1 = fs.Batch(tuning=(4, 16))
+    i1 = b1.add(rd)
+    b1.step(7)
+    alone = b1.state(i1)
+    b2 = fs.Batch(tuning=(4, 16))
+    i2 = b2.add(rd)
+    io = [b2.add(d) for d in others]
+    b2.step(7)
+    assert b2.stats()["graph_steps"] > 0
+    for k in alone:
+        assert np.array_equal(alone[k], b2.state(i2)[k]), k
+    b3 = fs.Batch(tuning=(4, 16))
+    io3 = [b3.add(d) for d in others]
+    b3.step(7)
+    for a, c in zip(io, io3):
+        for k in ("xs", "ps", "es"):
+            assert np.array_equal(b2.state(a)[k], b3.state(c)[k]), k
+    for b in (b1, b2, b3):
+        b.close()

@@ -218,3 +218,64 @@ def test_adaptive_fp32c_session_runs_with_refinement():
     a, b = g32.state(), g64.state()
     assert len(a["xs"]) == len(b["xs"])
     assert rel(a["es"], b["es"]) < 1e-5
+
+
+def test_relativistic_push_steps_bit_identical():
+    """The opt-in relativistic push (relativistic_momentum_push's velocity
+    (p/m)/sqrt(1 + (p/m)^2) in every RK4 stage) on the two-species Landau deck:
+    device steps equal the oracle's bit for bit before the first remesh, and
+    the push changes the trajectory."""
+    d = decks.landau_two_species(h=4, ph=1)
+    d["relativistic_push"] = 1
+    g, o = M.Simulation(d), O.Sim(d)
+    for _ in range(4):
+        g.step()
+        o.step()
+        a, b = g.state(), o.state()
+        for k in ("xs", "ps", "q_ws", "es"):
+            assert np.array_equal(a[k], b[k]), k
+    d["relativistic_push"] = 0
+    n = O.Sim(d)
+    n.step(4)
+    assert rel(g.state()["xs"], n.state()["xs"]) > 1e-6
+
+
+def test_relativistic_two_stream_session_matches_oracle():
+    """ics 7 (boosted Maxwell-Juttner pair) with the relativistic push through
+    two remeshes.  The initial f equals the library's host f0 at the mesh
+    points bit for bit; against the oracle, whose K_1 is its own quadrature,
+    it agrees to 1e-14, and so the trajectory agrees to rounding."""
+    d = decks.relativistic_two_stream(h=4, ph=1, steps=12)
+    g, o = M.Simulation(d, "direct64"), O.Sim(d)
+    a, b = g.state(), o.state()
+    assert np.array_equal(a["xs"], b["xs"]) and np.array_equal(a["ps"], b["ps"])
+    assert np.array_equal(a["fs"], M.initial_f0(d, 0, a["xs"], a["ps"]))
+    assert rel(a["fs"], b["fs"]) < 1e-14
+    for step in range(12):
+        g.step()
+        o.step()
+        a, b = g.state(), o.state()
+        for k in ("xs", "ps", "fs", "es"):
+            assert rel(a[k], b[k]) < 1e-11, (step, k)
+    assert np.max(np.abs(np.diff(a["xs"]))) > 0 and np.max(np.abs(a["ps"])) > 1.0
+
+
+@pytest.mark.parametrize("ics,keys,dom", [
+    (5, {"pth": 0.5, "amp": 0.02}, (-0.001, 0.001)),
+    (6, {"mu": 2.0, "amp": 0.01}, (0.0, 4 * np.pi)),
+    (8, {"amp": 1.3, "wave_beta": 0.8, "pth": 0.3}, (0.0, 5.0)),
+])
+def test_boost_initial_conditions_in_session(ics, keys, dom):
+    """Friedman beam, Maxwell-Juttner and travelling-wave initial conditions
+    build a session whose initial f is the host f0 at its mesh points, and
+    which steps."""
+    d = dict(xmin=dom[0], xmax=dom[1], dt=0.05, greens_epsilon=0.05, remesh_period=5, quadrature=0,
+             species_list=[dict(name="e", ics_type=ics, q=-1.0, m=1.0, initial_height=4, p_height=1,
+                                pmin=-3.0, pmax=3.0, **keys)])
+    g = M.Simulation(d, "direct64")
+    a = g.state()
+    assert np.array_equal(a["fs"], M.initial_f0(d, 0, a["xs"], a["ps"]))
+    assert np.array_equal(a["fs"], O.initial_f0(d, 0, a["xs"], a["ps"])) or ics != 5
+    g.step(2)
+    assert np.all(np.isfinite(g.state()["xs"]))
+    g.close()

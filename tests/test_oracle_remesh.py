@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from multi_species_b200 import decks
 
 
 def landau(x, p):
@@ -74,3 +75,37 @@ def test_field_energy_formula():
     x = np.linspace(0, L, 65)[:-1]
     e = np.sin(x)
     assert abs(O.field_energy(x, e, L) - 0.5 * np.pi) < 1e-12
+
+
+def test_adaptive_session_start_and_remesh():
+    """The oracle session with adaptive refinement: its initial state is the
+    adaptive mesh builder's (f0 at every point, new ones included), and it
+    steps through two remeshes, refining again at each."""
+    d = decks.two_stream(h=3, ph=1, steps=6, remesh_period=3)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=5, amr_epsilons=[0.02])
+    sp = d["species_list"][0]
+    xs, ps, f, _, _ = O.adaptive_mesh(3, 1, d["xmin"], d["xmax"], sp["pmin"], sp["pmax"],
+                                      (sp["ics_type"], sp["pth"], sp["pstr"], sp["amp"], 1.0), [0.02], 5)
+    s = O.Sim(d)
+    st = s.state()
+    assert len(st["xs"]) == len(xs) > 17 * 33
+    assert np.array_equal(st["xs"], xs) and np.array_equal(st["ps"], ps) and np.array_equal(st["fs"], f)
+    for _ in range(6):
+        s.step()
+        st = s.state()
+        assert len(st["xs"]) > 17 * 33 and np.all(np.isfinite(st["fs"])) and np.all(np.isfinite(st["es"]))
+
+
+def test_relativistic_push_respects_the_speed_limit():
+    """With the opt-in relativistic push every point moves less than c dt per
+    step (|v| = |p|/sqrt(1 + p^2) < 1 for m = 1); without it points with
+    |p| > 1 move further."""
+    d = decks.relativistic_two_stream(h=3, ph=1, steps=1)
+    s = O.Sim(d)
+    x0 = s.state()["xs"]
+    s.step()
+    assert np.max(np.abs(s.state()["xs"] - x0)) < d["dt"]
+    d["relativistic_push"] = 0
+    n = O.Sim(d)
+    n.step()
+    assert np.max(np.abs(n.state()["xs"] - x0)) > 2 * d["dt"]
