@@ -526,28 +526,51 @@ def run_serve(a, rank, world, local_rank):
                             "end to end by construction"}}
 
 
-def host_rk4_step(field, xs, ps, es, qw, qm, dt):
+def host_rk4_step(field, xs, ps, es, qw, qm, dt, work=None):
     """AMRSimulation::rk4_step + end-of-step field on the host, each field
-    evaluation through the plugin call with host arrays (qm per point)."""
+    evaluation through the plugin call with host arrays (qm per point).  The
+    caller's arithmetic is the reference's, in its order, written in place
+    into preallocated buffers (`work`, nine arrays of len(xs)) the way the
+    reference's C++ loops write into its vectors."""
     n = len(xs)
-    ef1 = es * qm
-    p2 = ps + 0.5 * dt * ef1
-    xk = xs + 0.5 * dt * ps
-    ef2 = np.empty(n)
+    if work is None:
+        work = [np.empty(n) for _ in range(9)]
+    ef1, ef2, ef3, ef4, p2, p3, p4, xk, tmp = work
+    mul, add = np.multiply, np.add
+    mul(es, qm, out=ef1)
+    mul(0.5 * dt, ef1, out=p2)
+    add(ps, p2, out=p2)
+    mul(0.5 * dt, ps, out=xk)
+    add(xs, xk, out=xk)
     field(ef2, xk, n, xk, qw, n)
-    ef2 *= qm
-    p3 = ps + 0.5 * dt * ef2
-    xk = xs + 0.5 * dt * p2
-    ef3 = np.empty(n)
+    mul(ef2, qm, out=ef2)
+    mul(0.5 * dt, ef2, out=p3)
+    add(ps, p3, out=p3)
+    mul(0.5 * dt, p2, out=xk)
+    add(xs, xk, out=xk)
     field(ef3, xk, n, xk, qw, n)
-    ef3 *= qm
-    p4 = ps + dt * ef3
-    xk = xs + dt * p3
-    ef4 = np.empty(n)
+    mul(ef3, qm, out=ef3)
+    mul(dt, ef3, out=p4)
+    add(ps, p4, out=p4)
+    mul(dt, p3, out=xk)
+    add(xs, xk, out=xk)
     field(ef4, xk, n, xk, qw, n)
-    ef4 *= qm
-    xs = xs + dt / 6.0 * (ps + 2 * p2 + 2 * p3 + p4)
-    ps = ps + dt / 6.0 * (ef1 + 2 * ef2 + 2 * ef3 + ef4)
+    mul(ef4, qm, out=ef4)
+    # xs + dt/6 (p1 + 2 p2 + 2 p3 + p4) and ps + dt/6 (ef1 + 2 ef2 + 2 ef3 + ef4), left to right
+    mul(2, p2, out=tmp)
+    add(ps, tmp, out=tmp)
+    mul(2, p3, out=xk)
+    add(tmp, xk, out=tmp)
+    add(tmp, p4, out=tmp)
+    mul(dt / 6.0, tmp, out=tmp)
+    xs = xs + tmp
+    mul(2, ef2, out=tmp)
+    add(ef1, tmp, out=tmp)
+    mul(2, ef3, out=xk)
+    add(tmp, xk, out=tmp)
+    add(tmp, ef4, out=tmp)
+    mul(dt / 6.0, tmp, out=tmp)
+    ps = ps + tmp
     es = np.empty(n)
     field(es, xs, n, xs, qw, n)
     return xs, ps, es
@@ -568,11 +591,12 @@ def e2e_plugin(deck, field_kind, n, device):
         f = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], prec, device=device)
     qm = np.concatenate([np.full(c, sp["q"] / sp["m"]) for c, sp in zip(counts, deck["species_list"])])
     xs, ps, es, qw = st["xs"], st["ps"], st["es"], st["q_ws"]
-    xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"])  # warm-up
+    work = [np.empty(len(xs)) for _ in range(9)]
+    xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"], work)  # warm-up
     steps = 2
     t0 = time.perf_counter()
     for _ in range(steps):
-        xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"])
+        xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"], work)
     dt = time.perf_counter() - t0
     f.close()
     pairs = 4.0 * n * n * steps

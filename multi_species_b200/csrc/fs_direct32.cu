@@ -341,7 +341,10 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
                 acc2[h] = make_float2(0.f, 0.f);
             }
-#pragma unroll 4
+            // eight sources per unrolled body: 32 independent reciprocal
+            // chains per thread keep MUFU and the FP32 pipe fed together
+            // (unroll 4 measured 3.5% slower, 16 no faster)
+#pragma unroll 8
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
                 const float2 sx2 = make_float2(e.x, e.x);
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
 // items in chunk-major order from an atomic counter, so the last, shorter
 // chunk comes last and no SM idles through a partial final wave.
 template <int kR>
-__global__ void __launch_bounds__(kNT) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
+__global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
                                                             int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
     __shared__ __align__(8) uint64_t bar[2];

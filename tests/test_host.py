@@ -83,3 +83,32 @@ def test_session_rejects_open_boundaries_and_bad_drive():
     with pytest.raises(M.FsError) as e:
         M.Simulation(d2)
     assert e.value.code == 1
+
+
+def test_bench_host_rk4_caller_is_the_references_step():
+    """The end-to-end leg of bench.py emulates AMRSimulation::rk4_step calling
+    the field plugin with host arrays; with the oracle's direct sum as the
+    plugin it reproduces the oracle's step bit for bit."""
+    import importlib.util
+    import pathlib
+
+    import oracle as O
+    from multi_species_b200 import decks
+    spec = importlib.util.spec_from_file_location("bench", pathlib.Path(__file__).resolve().parents[1] / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    d = decks.landau_two_species(h=3, ph=1)
+    d["remesh_period"] = 100
+    o = O.Sim(d)
+    st = o.state()
+    L = d["xmax"] - d["xmin"]
+    counts = o.species_points
+    qm = np.concatenate([np.full(c, sp["q"] / sp["m"]) for c, sp in zip(counts, d["species_list"])])
+
+    def field(es, t, nt, s, q, ns):
+        es[:] = O.direct_sum(L, d["greens_epsilon"], t[:nt], s[:ns], q[:ns])
+
+    xs, ps, es = bench.host_rk4_step(field, st["xs"], st["ps"], st["es"], st["q_ws"], qm, d["dt"])
+    o.step()
+    b = o.state()
+    assert np.array_equal(xs, b["xs"]) and np.array_equal(ps, b["ps"]) and np.array_equal(es, b["es"])
