@@ -591,17 +591,27 @@ def e2e_plugin(deck, field_kind, n, device):
         f = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], prec, device=device)
     qm = np.concatenate([np.full(c, sp["q"] / sp["m"]) for c, sp in zip(counts, deck["species_list"])])
     xs, ps, es, qw = st["xs"], st["ps"], st["es"], st["q_ws"]
+    in_calls = [0.0]
+
+    def timed_field(*args):
+        c0 = time.perf_counter()
+        f(*args)
+        in_calls[0] += time.perf_counter() - c0
+
     work = [np.empty(len(xs)) for _ in range(9)]
-    xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"], work)  # warm-up
+    xs, ps, es = host_rk4_step(timed_field, xs, ps, es, qw, qm, deck["dt"], work)  # warm-up
     steps = 2
+    in_calls[0] = 0.0
     t0 = time.perf_counter()
     for _ in range(steps):
-        xs, ps, es = host_rk4_step(f, xs, ps, es, qw, qm, deck["dt"], work)
+        xs, ps, es = host_rk4_step(timed_field, xs, ps, es, qw, qm, deck["dt"], work)
     dt = time.perf_counter() - t0
     f.close()
     pairs = 4.0 * n * n * steps
     return {"value": pairs / dt, "unit": "pair-interactions/s", "h2d_bytes_per_step": 4 * 16 * n,
             "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
+            "ms_per_plugin_call": 1e3 * in_calls[0] / (4 * steps),
+            "host_rk4_ms_per_step": 1e3 * (dt - in_calls[0]) / steps,
             "path": f"{type(f).__name__}(es, targets, nt, sources, q_ws, ns) with host arrays, host RK4"}
 
 
