@@ -305,7 +305,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 acc2[h] = make_float2(0.f, 0.f);
                 ncmp2[h] = make_float2(0.f, 0.f);
             }
-#pragma unroll 2
+#pragma unroll 4
             for (int j = 0; j < kS; ++j) {
                 const float4 e = tile[j];
                 const float2 sx2 = make_float2(e.x, e.x);
