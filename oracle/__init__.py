@@ -164,6 +164,7 @@ def adaptive_mesh(h, ph, xmin, xmax, pmin, pmax, f0_params, amr_eps, max_height,
     panels (n x 18), leaves)."""
     m = Mesh(h, ph, xmin, xmax, pmin, pmax)
     ics, pth, pstr, amp, nk = f0_params
+    _stateless_ics(ics)
     kx = 2 * np.pi / ((xmax - xmin) if L is None else L) * nk
     n = m.npoints
     f = np.array([lib().fso_f0(ics, pth, pstr, kx, amp, x, p) for x, p in zip(m.xs, m.ps)])
@@ -299,7 +300,15 @@ class Mesh:
             self._m = None
 
 
+def _stateless_ics(ics):
+    """fso_f0 holds the closed forms (ics 1-4, 9, 10 and the Landau default);
+    the tabulated and Bessel-normalised forms need initial_f0's parameters."""
+    if int(ics) in (5, 6, 7, 8):
+        raise ValueError(f"ics_type {ics} needs initial_f0(deck, species, x, p)")
+
+
 def f0(ics, pth, pstr, k, amp, x, p):
+    _stateless_ics(ics)
     fn = lib().fso_f0
     return np.array([fn(ics, pth, pstr, k, amp, float(a), float(b)) for a, b in zip(x, p)])
 

@@ -103,3 +103,10 @@ def test_invalid_initial_conditions_are_rejected(sp, xr, x):
     assert e.value.code == 1
     with pytest.raises(ValueError):
         O.initial_f0(d, 0, np.array([x]), np.array([0.1]))
+
+
+def test_stateless_oracle_helpers_refuse_tabulated_forms():
+    for ics in (5, 6, 7, 8):
+        with pytest.raises(ValueError):
+            O.f0(ics, 1.0, 0.0, 0.5, 0.01, [0.1], [0.2])
+    assert O.f0(1, 1.0, 0.0, 0.5, 0.01, [0.1], [0.2])[0] > 0
