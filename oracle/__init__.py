@@ -25,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(HERE, "liboracle.so")
 _REF = os.path.join(HERE, "_ref", "libfs_ref.so")
+_AMR_REF = os.path.join(HERE, "_ref", "libamr_ref.so")
 PANEL_INTS = 18
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -59,6 +60,7 @@ class FsoSim(C.Structure):
 
 _lib = None
 _ref = None
+_amr_ref = None
 
 
 def lib():
@@ -143,6 +145,50 @@ def ref():
         R.fsref_treecode.restype = C.c_int
         _ref = R
     return _ref
+
+
+def amr_ref_available() -> bool:
+    return os.path.exists(_AMR_REF)
+
+
+def amr_ref():
+    """The reference's own simulation code (oracle/_ref/libamr_ref.so: every
+    source of src/structure_files, src/simulation_files and src/FieldStructure.cpp
+    with amr_harness.cpp)."""
+    global _amr_ref
+    if _amr_ref is None:
+        if not os.path.exists(_AMR_REF):
+            raise FileNotFoundError(f"{_AMR_REF} missing: run `make -C oracle REF=<reference checkout>`")
+        R = C.CDLL(_AMR_REF)
+        R.amrref_sim_create.argtypes = [C.c_char_p, C.c_char_p]
+        R.amrref_sim_create.restype = C.c_void_p
+        R.amrref_sim_destroy.argtypes = [C.c_void_p]
+        R.amrref_sim_step.argtypes = [C.c_void_p, C.c_int]
+        R.amrref_sim_step.restype = C.c_int
+        for n in ("amrref_sim_remesh", "amrref_sim_nspecies"):
+            getattr(R, n).argtypes = [C.c_void_p]
+            getattr(R, n).restype = C.c_int
+        for n in ("amrref_sim_species_points", "amrref_sim_npanels", "amrref_sim_nleaves", "amrref_sim_nreduced"):
+            getattr(R, n).argtypes = [C.c_void_p, C.c_int]
+            getattr(R, n).restype = C.c_int
+        R.amrref_sim_iter.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        R.amrref_sim_iter.restype = C.c_int
+        R.amrref_sim_state.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+        R.amrref_sim_state.restype = C.c_int
+        R.amrref_sim_set_xp.argtypes = [C.c_void_p, _dp, _dp]
+        R.amrref_sim_set_xp.restype = C.c_int
+        R.amrref_sim_panels.argtypes = [C.c_void_p, C.c_int, _ip]
+        R.amrref_sim_panels.restype = C.c_int
+        R.amrref_sim_leaves.argtypes = [C.c_void_p, C.c_int, _ip]
+        R.amrref_sim_leaves.restype = C.c_int
+        R.amrref_sim_reduced.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        R.amrref_sim_reduced.restype = C.c_int
+        R.amrref_sim_f_beyond.argtypes = [C.c_void_p, C.c_int]
+        R.amrref_sim_f_beyond.restype = C.c_double
+        R.amrref_sim_f0.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]
+        R.amrref_sim_f0.restype = C.c_int
+        _amr_ref = R
+    return _amr_ref
 
 
 def _f64(a):
@@ -450,3 +496,113 @@ def field_energy(xs, es, L):
     mx, me = x_sort[keep], e_sort[keep]
     dxs = 0.5 * np.hstack([mx[1] + L - mx[-1], mx[2:] - mx[:-2], mx[0] + L - mx[-2]])
     return 0.5 * float(np.dot(dxs, me ** 2))
+
+
+# ---------------------------------------------------------------- the reference simulation
+class RefSim:
+    """The reference's AMRSimulation (oracle/_ref/libamr_ref.so), built from a
+    deck dict exactly as run_FARRSIGHT2.cpp builds it from deck.json: the deck
+    is written as JSON into a fresh simulation directory holding the output
+    folders the reference writes to (simulation_output/<species>/{xs,ps,fs,
+    panels} and simulation_output/{reduce_xs,reduced_es}), then stepped with
+    AMRSimulation::step.  `sim_dir` keeps the reference's dump files for
+    comparisons; by default a temporary directory removed on close."""
+
+    def __init__(self, deck: dict, sim_dir: str | None = None):
+        import json
+        import tempfile
+        self._s = None
+        self._tmp = None
+        if sim_dir is None:
+            self._tmp = tempfile.TemporaryDirectory(prefix="amrref_")
+            sim_dir = self._tmp.name
+        self.sim_dir = os.path.join(os.path.abspath(sim_dir), "")
+        out = os.path.join(self.sim_dir, "simulation_output")
+        for sp in deck["species_list"]:
+            for sub in ("xs", "ps", "fs", "panels"):
+                os.makedirs(os.path.join(out, sp["name"], sub), exist_ok=True)
+        for sub in ("reduce_xs", "reduced_es"):
+            os.makedirs(os.path.join(out, sub), exist_ok=True)
+        self.deck_path = os.path.join(self.sim_dir, "deck.json")
+        with open(self.deck_path, "w") as f:
+            json.dump(deck, f)
+        R = amr_ref()
+        self._s = R.amrref_sim_create(self.sim_dir.encode(), self.deck_path.encode())
+        if not self._s:
+            raise ValueError("the reference rejected the deck")
+        self.nspecies = R.amrref_sim_nspecies(self._s)
+
+    @property
+    def species_points(self):
+        return [amr_ref().amrref_sim_species_points(self._s, i) for i in range(self.nspecies)]
+
+    @property
+    def n(self):
+        return int(sum(self.species_points))
+
+    def step(self, n=1):
+        if amr_ref().amrref_sim_step(self._s, int(n)):
+            raise RuntimeError("reference step raised")
+
+    def remesh(self):
+        if amr_ref().amrref_sim_remesh(self._s):
+            raise RuntimeError("reference remesh raised")
+
+    @property
+    def iter(self):
+        return amr_ref().amrref_sim_iter(self._s, None)
+
+    @property
+    def t(self):
+        t = C.c_double()
+        amr_ref().amrref_sim_iter(self._s, C.byref(t))
+        return t.value
+
+    def state(self):
+        a = {k: np.zeros(self.n) for k in ("xs", "ps", "fs", "q_ws", "es")}
+        amr_ref().amrref_sim_state(self._s, *(a[k].ctypes.data for k in ("xs", "ps", "fs", "q_ws", "es")))
+        return a
+
+    def set_xp(self, xs, ps):
+        amr_ref().amrref_sim_set_xp(self._s, _f64(xs), _f64(ps))
+
+    def panels(self, species):
+        R = amr_ref()
+        out = np.zeros((R.amrref_sim_npanels(self._s, species), PANEL_INTS), dtype=np.int32)
+        R.amrref_sim_panels(self._s, species, out)
+        return out
+
+    def leaves(self, species):
+        R = amr_ref()
+        out = np.zeros(R.amrref_sim_nleaves(self._s, species), dtype=np.int32)
+        R.amrref_sim_leaves(self._s, species, out)
+        return out
+
+    def reduced(self, species):
+        """(unique x, summed weights, reduced E) of the species' last reduced grid."""
+        R = amr_ref()
+        u = R.amrref_sim_nreduced(self._s, species)
+        rx, rw, re = np.zeros(u), np.zeros(u), np.zeros(u)
+        R.amrref_sim_reduced(self._s, species, rx.ctypes.data, rw.ctypes.data, re.ctypes.data)
+        return rx, rw, re
+
+    def f_beyond_boundary(self, species):
+        return amr_ref().amrref_sim_f_beyond(self._s, species)
+
+    def f0(self, species, x, p):
+        x, p = _f64(x), _f64(p)
+        out = np.zeros(len(x))
+        if amr_ref().amrref_sim_f0(self._s, species, len(x), x, p, out):
+            raise RuntimeError("reference initial condition raised")
+        return out
+
+    def close(self):
+        if getattr(self, "_s", None):
+            amr_ref().amrref_sim_destroy(self._s)
+            self._s = None
+        if getattr(self, "_tmp", None):
+            self._tmp.cleanup()
+            self._tmp = None
+
+    def __del__(self):
+        self.close()
