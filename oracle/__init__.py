@@ -1,15 +1,21 @@
 """CPU oracle for the FARRSIGHT per-step hot path -- TEST INFRASTRUCTURE ONLY.
 
-Two libraries, both built by ``oracle/Makefile``:
+Three libraries, all built by ``oracle/Makefile``:
 
 * ``oracle/_ref/libfs_ref.so`` -- the reference's own ``src/FieldStructure.cpp``
   compiled unmodified (direct sum ``src/FieldStructure.cpp:102-156`` and treecode
   ``:230-1020``).  This is the pin for the field.
+* ``oracle/_ref/libamr_ref.so`` -- every source of the reference's simulation
+  (``src/structure_files``, ``src/simulation_files``, ``src/FieldStructure.cpp``)
+  compiled unmodified, with stand-ins for the Eigen / Boost calls it makes
+  (``oracle/refshim``), driven through ``amr_harness.cpp``.  This is the pin for
+  the mesh, RK4, step control, remesh, reduced grid, adaptive refinement and
+  initial conditions.
 * ``oracle/liboracle.so`` -- ``fs_oracle.c``, a plain C restatement of the whole
-  hot path (field, treecode, panel mesh, remesh, RK4 step control).  Its field
-  functions are checked bit for bit against the reference library; the mesh /
-  remesh / RK4 parts are PARITY UNPINNED (their reference files cannot be
-  compiled here: absolute Boost include paths and Eigen).
+  hot path (field, treecode, panel mesh, remesh, RK4 step control), checked bit
+  for bit against both reference libraries.  Its 9x9 solve and the Eigen
+  stand-in share the same partial-pivot LU; against Eigen itself the remesh fit
+  agrees to rounding.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline / reference arm
 of ``bench.py`` may import this package.  The product never does.

@@ -7,12 +7,12 @@
  *
  * Pinning: the field functions (fso_direct_sum, fso_treecode) are checked
  * against the reference's own src/FieldStructure.cpp compiled unmodified into
- * oracle/_ref/libfs_ref.so.  The mesh / remesh / RK4 / reduced-grid parts live
- * in reference files that cannot be compiled here (they #include Boost headers
- * by absolute path and need Eigen), so for those parts PARITY IS UNPINNED: they
- * are a faithful restatement checked by invariants (exact quadratic
- * reproduction, identity remesh, charge conservation) rather than by reference
- * outputs.
+ * oracle/_ref/libfs_ref.so.  The mesh, remesh, RK4, step control, reduced
+ * grid, adaptive refinement and initial conditions are checked bit for bit
+ * against the reference's own AMRStructure / AMRSimulation sources compiled
+ * into oracle/_ref/libamr_ref.so (with stand-ins for the Eigen and Boost calls
+ * they make, oracle/refshim).  The 9x9 solve here and the Eigen stand-in use
+ * the same partial-pivot LU; against Eigen itself the fits agree to rounding.
  */
 #ifndef FS_ORACLE_H
 #define FS_ORACLE_H

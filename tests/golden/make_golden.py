@@ -7,10 +7,13 @@ field_*.npz, drive_fields.npz -- inputs and outputs of the REFERENCE's own
     (ExternalTanh / ExternalSine / ExternalLogistic) (src/FieldStructure.cpp),
     run through oracle/_ref/libfs_ref.so (built from the reference sources by
     oracle/Makefile).  These pin the field.
-sim_landau_h3.npz -- a short two-species trajectory (3 panels deep, 6 steps,
-    one remesh) of the C oracle restatement (oracle/liboracle.so).  The
-    reference's simulation driver cannot be compiled here, so this fixture
-    records the restatement (parity unpinned) and guards it against drift.
+sim_landau_h3.npz, ref_sim_*.npz -- trajectories of the REFERENCE's own
+    AMRSimulation (constructor from the deck, then step(); src/simulation_files,
+    src/structure_files, src/FieldStructure.cpp) run through
+    oracle/_ref/libamr_ref.so, built from the reference sources by
+    oracle/Makefile: the state (xs, ps, fs, q_ws, es, species concatenated) at
+    the listed iterations.  These pin RK4, step control, the remesh, the
+    reduced grid, adaptive refinement and the treecode session.
 
 Inputs are seeded; every array is float64.
 """
@@ -80,17 +83,46 @@ def main():
     e = O.ref_treecode(L, 0.02, 0.7, 8, 300, x, q)
     np.savez_compressed(os.path.join(HERE, "field_treecode.npz"), L=L, eps=0.02, mac=0.7, degree=8,
                         max_source=300, sources=x, q=q, es=e)
-    deck = decks.landau_two_species(h=3, ph=1, steps=6)
-    s = O.Sim(deck)
-    traj = {}
-    for k in range(7):
-        st = s.state()
-        for key in ("xs", "ps", "fs", "q_ws", "es"):
-            traj[f"{key}_{k}"] = st[key]
-        if k < 6:
-            s.step()
-    np.savez_compressed(os.path.join(HERE, "sim_landau_h3.npz"), **traj)
+    if not O.amr_ref_available():
+        raise SystemExit("oracle/_ref/libamr_ref.so missing: run `make -C oracle REF=<reference checkout>`")
+    save_trajectory("sim_landau_h3.npz", decks.landau_two_species(h=3, ph=1, steps=6), range(7))
+    for name, (deck, iters) in REF_TRAJECTORIES.items():
+        save_trajectory(f"ref_sim_{name}.npz", deck, iters)
     print("golden fixtures written to", HERE)
+
+
+def _adaptive_two_stream():
+    d = decks.two_stream(h=3, ph=1, steps=6, remesh_period=3)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=5, amr_epsilons=[0.02])
+    return d
+
+
+def _bump_on_tail_treecode():
+    d = decks.bump_on_tail(h=3, ph=1, steps=6)
+    d["max_source"] = 200
+    d["remesh_period"] = 3
+    return d
+
+
+# name -> (deck, iterations whose state is stored)
+REF_TRAJECTORIES = {
+    "two_stream_h4": (decks.two_stream(h=4, ph=1, steps=8, remesh_period=3), (0, 2, 3, 6, 8)),
+    "adaptive_two_stream_h3": (_adaptive_two_stream(), (0, 2, 3, 6)),
+    "bump_on_tail_h3": (_bump_on_tail_treecode(), (0, 2, 3, 6)),
+}
+
+
+def save_trajectory(fname, deck, iters):
+    """The reference's state at each iteration of `iters` (increasing)."""
+    r = O.RefSim(deck)
+    out = {"iters": np.array(list(iters), dtype=np.int32)}
+    for k in iters:
+        r.step(k - r.iter)
+        st = r.state()
+        for key in ("xs", "ps", "fs", "q_ws", "es"):
+            out[f"{key}_{k}"] = st[key]
+    r.close()
+    np.savez_compressed(os.path.join(HERE, fname), **out)
 
 
 if __name__ == "__main__":

@@ -1,5 +1,6 @@
-"""The oracle pinned against the reference: its own field solvers compiled from
-the reference sources (oracle/_ref) and the golden fixtures they produced."""
+"""The oracle pinned against the reference: its own field solvers and
+simulation compiled from the reference sources (oracle/_ref) and the golden
+fixtures they produced."""
 import glob
 import os
 
@@ -91,12 +92,35 @@ def test_treecode_normalisation_vs_direct():
     assert np.linalg.norm(t - d) / np.linalg.norm(d) < 1e-5
 
 
-def test_sim_trajectory_golden():
-    g = np.load(os.path.join(GOLD, "sim_landau_h3.npz"))
-    s = O.Sim(decks.landau_two_species(h=3, ph=1, steps=6))
-    for k in range(7):
+def _adaptive_two_stream():
+    d = decks.two_stream(h=3, ph=1, steps=6, remesh_period=3)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=5, amr_epsilons=[0.02])
+    return d
+
+
+def _bump_on_tail_treecode():
+    d = decks.bump_on_tail(h=3, ph=1, steps=6)
+    d["max_source"] = 200
+    d["remesh_period"] = 3
+    return d
+
+
+SIM_FIXTURES = {
+    "sim_landau_h3.npz": decks.landau_two_species(h=3, ph=1, steps=6),
+    "ref_sim_two_stream_h4.npz": decks.two_stream(h=4, ph=1, steps=8, remesh_period=3),
+    "ref_sim_adaptive_two_stream_h3.npz": _adaptive_two_stream(),
+    "ref_sim_bump_on_tail_h3.npz": _bump_on_tail_treecode(),
+}
+
+
+@pytest.mark.parametrize("fixture", sorted(SIM_FIXTURES))
+def test_sim_trajectory_matches_reference_golden_bitwise(fixture):
+    """Trajectories of the reference's AMRSimulation (remeshes, adaptive
+    refinement and the treecode included) against the restatement's session."""
+    g = np.load(os.path.join(GOLD, fixture))
+    s = O.Sim(SIM_FIXTURES[fixture])
+    for k in [int(i) for i in g["iters"]]:
+        s.step(k - s.iter)
         st = s.state()
         for key in ("xs", "ps", "fs", "q_ws", "es"):
             assert np.array_equal(st[key], g[f"{key}_{k}"]), (k, key)
-        if k < 6:
-            s.step()

@@ -1,0 +1,192 @@
+"""The C restatement of the simulation (oracle/fs_oracle.c) pinned to the
+reference's own simulation code, compiled from its sources into
+oracle/_ref/libamr_ref.so (AMRStructure_*.cpp, AMRSimulation_*.cpp,
+FieldStructure.cpp with the Eigen / Boost shims of oracle/refshim).
+
+Mesh construction, point order and panel links (AMRStructure_amr.cpp:127-839),
+f0 and weights (:1084-1151), RK4 and step control (AMRSimulation_step.cpp:5-263),
+remesh shifts, point location and the 9x9 fits (AMRStructure_interp.cpp:12-975),
+the reduced grid (AMRStructure.cpp:147-196), adaptive refinement
+(AMRStructure_amr.cpp:841-1081) and the initial conditions
+(initial_distributions.cpp) are compared state by state.  The restatement's
+9x9 solve follows the same partial-pivot LU as the Eigen shim, so the two
+agree bit for bit; against Eigen itself the fit agrees to rounding."""
+import numpy as np
+import pytest
+
+import oracle as O
+import multi_species_b200 as M
+from multi_species_b200 import decks
+
+pytestmark = pytest.mark.skipif(not O.amr_ref_available(), reason="reference simulation library not built")
+
+KEYS = ("xs", "ps", "fs", "q_ws", "es")
+
+
+def _landau():
+    return decks.landau_two_species(h=3, ph=1, steps=12)
+
+
+def _two_stream():
+    return decks.two_stream(h=4, ph=1, steps=8, remesh_period=3)
+
+
+def _simpson_ion_acoustic():
+    d = decks.landau_two_species(h=3, ph=1, steps=8)
+    d["quadrature"] = 1
+    d["species_list"][0].update(ics_type=9, pstr=0.5, amp=0.05)
+    d["species_list"][1].update(ics_type=10, amp=0.05)
+    return d
+
+
+def _colder_two_stream_driven():
+    d = decks.two_stream(h=3, ph=1, steps=8, remesh_period=4)
+    d["species_list"][0].update(ics_type=4, pth=0.5, pstr=2.0, amp=0.05)
+    d["external_field"] = {"use_external_field": 1, "external_type": 1, "Am": 0.4, "k": 0.2, "omega": 0.37}
+    return d
+
+
+def _long_walks():
+    """A long box (L = 20.5) with |v| up to 6: walks visit many panels."""
+    d = decks.landau_batch(count=2, seed=29, steps=10)[1]
+    for s in d["species_list"]:
+        s["initial_height"], s["p_height"] = min(s["initial_height"], 4), min(s["p_height"], 1)
+    return d
+
+
+def _treecode():
+    d = decks.bump_on_tail(h=3, ph=1, steps=6)
+    d["max_source"] = 200
+    d["remesh_period"] = 3
+    return d
+
+
+def _adaptive():
+    d = decks.two_stream(h=3, ph=1, steps=6, remesh_period=3)
+    d["species_list"][0].update(do_adaptively_refine=True, max_height=5, amr_epsilons=[0.02])
+    return d
+
+
+DECKS = {"landau_two_species": (_landau, 12), "two_stream": (_two_stream, 8),
+         "simpson_ion_acoustic": (_simpson_ion_acoustic, 8), "colder_two_stream_driven": (_colder_two_stream_driven, 8),
+         "long_walks": (_long_walks, 6), "treecode_bump_on_tail": (_treecode, 6), "adaptive_two_stream": (_adaptive, 6)}
+
+
+@pytest.mark.parametrize("name", sorted(DECKS))
+def test_trajectory_bit_identical_to_reference(name):
+    make, steps = DECKS[name]
+    d = make()
+    r, o = O.RefSim(d), O.Sim(d)
+    try:
+        for k in range(steps + 1):
+            if k:
+                r.step()
+                o.step()
+            a, b = r.state(), o.state()
+            assert r.iter == o.iter == k
+            assert len(a["xs"]) == len(b["xs"]), k
+            for key in KEYS:
+                assert np.array_equal(a[key], b[key]), (k, key)
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("h,ph,dom", [(2, 0, (0.0, 4 * np.pi, -6.0, 6.0)), (3, 1, (0.0, 10 * np.pi, -8.0, 8.0)),
+                                      (4, 2, (-1.0, 3.0, -2.0, 5.0))])
+def test_mesh_panels_and_leaves_match_reference(h, ph, dom):
+    xmin, xmax, pmin, pmax = dom
+    d = dict(xmin=xmin, xmax=xmax, dt=0.1, greens_epsilon=0.1, quadrature=0, num_steps=1,
+             species_list=[dict(name="e", ics_type=1, pth=1.0, amp=0.01, q=-1.0, m=1.0, initial_height=h,
+                                p_height=ph, pmin=pmin, pmax=pmax)])
+    r = O.RefSim(d)
+    m = O.Mesh(h, ph, xmin, xmax, pmin, pmax)
+    try:
+        st = r.state()
+        assert np.array_equal(st["xs"], m.xs) and np.array_equal(st["ps"], m.ps)
+        assert np.array_equal(r.panels(0), m.panels)
+        assert np.array_equal(r.leaves(0), m.leaves)
+        assert np.array_equal(st["q_ws"], m.base_weights(-1.0, 0) * st["fs"])
+    finally:
+        r.close()
+
+
+def test_reduced_grid_matches_reference():
+    d = _landau()
+    r = O.RefSim(d)
+    try:
+        r.step(5)  # the remesh evaluates the field on the reduced grid
+        st = r.state()
+        off = 0
+        for s, n in enumerate(r.species_points):
+            rx, rw, _ = r.reduced(s)
+            ox, ow, inv = O.reduce(st["xs"][off:off + n], st["q_ws"][off:off + n])
+            assert np.array_equal(rx, ox) and np.array_equal(rw, ow)
+            _, _, re = r.reduced(s)
+            assert np.array_equal(st["es"][off:off + n], re[inv])
+            off += n
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("t,wiggle", [(0.7, 0.0), (2.5, 0.3), (6.0, 1.1)])
+def test_remesh_of_sheared_and_tangled_states_matches_reference(t, wiggle):
+    """Positions x + p t + wiggle sin(3 p) (large t and wiggle fold panels over
+    one another); the reference's shift, walk order and fits decide f."""
+    d = decks.two_stream(h=4, ph=1, steps=1, remesh_period=1000)
+    r = O.RefSim(d)
+    try:
+        st = r.state()
+        xs = st["xs"] + st["ps"] * t + wiggle * np.sin(3.0 * st["ps"])
+        r.set_xp(xs, st["ps"])
+        f_beyond = r.f_beyond_boundary(0)
+        r.remesh()
+        got = r.state()
+        sp = d["species_list"][0]
+        m = O.Mesh(4, 1, d["xmin"], d["xmax"], sp["pmin"], sp["pmax"])
+        nf, _, _ = m.remesh(xs, st["ps"], st["fs"], f_beyond)
+        assert np.array_equal(got["fs"], nf)
+        assert np.array_equal(got["xs"], m.xs)
+    finally:
+        r.close()
+
+
+IC_CASES = [
+    ("landau", {"ics_type": 1, "pth": 1.0, "amp": 0.05}, (0.0, 4 * np.pi), (-6, 6)),
+    ("strong_landau", {"ics_type": 2, "pth": 1.0, "pstr": 0.3, "amp": 0.5}, (0.0, 4 * np.pi), (-6, 6)),
+    ("strong_two_stream", {"ics_type": 3, "pth": 1.0, "amp": 0.005}, (0.0, 10 * np.pi), (-8, 8)),
+    ("colder_two_stream", {"ics_type": 4, "pth": 0.5, "pstr": 2.0, "amp": 0.05}, (0.0, 4 * np.pi), (-6, 6)),
+    ("friedman_beam", {"ics_type": 5, "pth": 1.0, "amp": 0.05}, (-2.0, 2.0), (-3, 3)),
+    ("maxwell_juttner", {"ics_type": 6, "mu": 2.0, "amp": 0.01}, (0.0, 4 * np.pi), (-8, 8)),
+    ("relativistic_two_stream", {"ics_type": 7, "mu": 30.0, "pstr": 1.0, "amp": 0.01}, (0.0, 4 * np.pi), (-4, 4)),
+    ("travelling_wave", {"ics_type": 8, "amp": 1.3, "wave_beta": 0.8, "pth": 0.3}, (0.0, 5.0), (-1.5, 1.5)),
+    ("ion_acoustic_electron", {"ics_type": 9, "pth": 1.0, "pstr": 0.5, "amp": 0.05}, (0.0, 4 * np.pi), (-6, 6)),
+    ("ion_acoustic_ion", {"ics_type": 10, "pth": 0.1, "amp": 0.05, "m": 100.0}, (0.0, 4 * np.pi), (-1, 1)),
+    ("unknown_is_landau", {"ics_type": 11, "pth": 1.0, "amp": 0.05}, (0.0, 4 * np.pi), (-6, 6)),
+]
+
+
+@pytest.mark.parametrize("name,sp,xr,pr", IC_CASES, ids=[c[0] for c in IC_CASES])
+def test_initial_conditions_match_reference(name, sp, xr, pr):
+    """The reference's distribution objects (built by make_f0_return_ptr from
+    the deck) against the restatement and the library's host f0.  K_1 and the
+    elliptic integrals come from the standard library behind the Boost shim,
+    as in the library, so the library agrees bit for bit everywhere; the
+    restatement's own special functions agree to 1e-13."""
+    spd = dict(dict(name="e", pmin=float(pr[0]), pmax=float(pr[1]), initial_height=2, p_height=0, q=-1.0, m=1.0),
+               **sp)
+    d = {"xmin": xr[0], "xmax": xr[1], "dt": 0.1, "greens_epsilon": 0.05, "quadrature": 0, "num_steps": 1,
+         "species_list": [spd]}
+    rng = np.random.default_rng(len(name))
+    x, p = rng.uniform(*xr, 2000), rng.uniform(*pr, 2000)
+    r = O.RefSim(d)
+    try:
+        ref = r.f0(0, x, p)
+    finally:
+        r.close()
+    assert np.all(np.isfinite(ref)) and np.max(ref) > 0
+    assert np.array_equal(M.initial_f0(d, 0, x, p), ref)
+    ora = O.initial_f0(d, 0, x, p)
+    if sp["ics_type"] in (6, 7, 8):
+        assert np.max(np.abs(ora - ref) / np.maximum(np.abs(ref), 1e-300)) <= 1e-13
+    else:
+        assert np.array_equal(ora, ref)

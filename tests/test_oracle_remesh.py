@@ -1,5 +1,5 @@
-"""Invariants of the remesh / mesh restatement (parity unpinned: the reference's
-AMRStructure sources cannot be compiled here)."""
+"""Invariants of the remesh / mesh restatement; its parity with the
+reference's own AMRStructure code is in tests/test_oracle_reference_sim.py."""
 import numpy as np
 import pytest
 
