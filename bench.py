@@ -2,7 +2,8 @@
 """Benchmark of the FARRSIGHT hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload two_stream|landau] [--field direct32c|direct64]
+                    [--workload two_stream|landau|bump_on_tail|landau_batch|serve]
+                    [--field direct32c|direct64|treecode32c|treecode64]
 
 A step is one AMRSimulation::step of the workload (RK4 with three field
 evaluations, then either the fourth field evaluation or the remesh + reduced
@@ -13,12 +14,20 @@ compensated direct sum -- with synthetic inputs generated from the deck.
 value     pair interactions per second over the timed steps (whole job: all
           ranks' pairs / max-over-ranks device time), CUDA events on the
           simulation's stream; L2 flushed (256 MiB write) between timed steps.
+accuracy  FP32c against the plain FP64 path on the same workload: relative L2
+          error of E on the final state, and the field-energy drift over an
+          FP32c and an FP64 session stepped side by side from t = 0.
+plain_fp64_gpu  the FP64 session's rate (k_direct64, the reference arithmetic
+          bit for bit), with its FP64-pipe roofline; speedup_vs_plain_fp64_gpu
+          is value over it.
+batch     64 seeded Landau instances stepped together: rate, p50/p99 step
+          latency, speed-up over the plain FP64 path.
 e2e       same metric through the reference-facing plugin call
           (E_MQ_DirectSum_B200.__call__, i.e. fs_field_eval with HOST arrays)
           driving a host-side RK4 step like AMRSimulation::rk4_step: every
           field call copies sources and weights host->device and E back.
-roofline  the pair kernel (k_pairs32): achieved pair rate per launch-time
-          against the MUFU reciprocal-square-root peak (one MUFU op per pair).
+roofline  the dominant pair kernel: achieved pair rate per launch time against
+          its FP32-pipe bound (and the one-MUFU-plus-8-FP32 convention).
 cpu_baseline  the reference's own E_MQ_DirectSum (oracle/_ref, compiled from
           the reference sources) on all host cores, on a bounded target sample.
 
@@ -65,6 +74,10 @@ def parse():
                     help="default: direct32c, treecode32c for bump_on_tail")
     ap.add_argument("--h", type=int, default=None, help="override the mesh height (small cases for profiling)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 shadow run (accuracy, plain FP64 rate)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch record")
+    ap.add_argument("--drift-steps", type=int, default=None,
+                    help="steps of the FP32c-vs-FP64 field-energy comparison (default: warmup + steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     return ap.parse_args()
@@ -165,15 +178,23 @@ def traffic_per_pair(kernel: str):
 
 
 def _lattice(deck, h_drop=0):
-    """All species' mesh points and weights of a deck (optionally h reduced)."""
-    import multi_species_b200 as M
+    """All species' mesh points and weights of a deck (optionally h reduced),
+    from the oracle's mesh restatement: the CPU legs load no product code."""
+    import oracle as O
     xs, qs = [], []
     for sp in deck["species_list"]:
-        m = M.mesh(max(1, sp["initial_height"] - h_drop), sp["p_height"], deck["xmin"], deck["xmax"], sp["pmin"],
-                   sp["pmax"], q=sp["q"], quadrature=deck["quadrature"])
-        xs.append(m["xs"] + 0.2 * m["ps"])
-        qs.append(m["base_weights"])
+        m = O.Mesh(max(1, sp["initial_height"] - h_drop), sp["p_height"], deck["xmin"], deck["xmax"], sp["pmin"],
+                   sp["pmax"])
+        xs.append(m.xs + 0.2 * m.ps)
+        qs.append(m.base_weights(sp["q"], deck["quadrature"]))
     return np.concatenate(xs), np.concatenate(qs)
+
+
+def workload_config(name, deck, n, world):
+    """The workload, the same dict on both arms; how an arm computes it (field
+    kind, L2 handling) goes in top-level keys."""
+    return {"workload": name, "points": int(n), "eps": deck["greens_epsilon"], "dt": deck["dt"],
+            "remesh_period": deck["remesh_period"], "parallelism": f"replicas{world}"}
 
 
 def cpu_baseline(deck, seconds: float, treecode: bool = False):
@@ -237,10 +258,9 @@ def run_reference(a, rank, world):
             # one RK4 step is four evaluations of n x n pairs; each timed step here
             # is a bounded sample of one evaluation, so the step time is extrapolated
             "ms_per_step": 4.0 * n * n / v * 1e3,
-            "config": {"workload": name, "points": n, "eps": deck["greens_epsilon"], "dt": deck["dt"],
-                       "remesh_period": deck["remesh_period"],
-                       "field": ("reference E_MQ_Treecode (CPU, serial as shipped)" if tree
-                                 else "reference E_MQ_DirectSum (CPU, OpenMP)")},
+            "config": workload_config(name, deck, n, world),
+            "field": ("reference E_MQ_Treecode (CPU, serial as shipped)" if tree
+                      else "reference E_MQ_DirectSum (CPU, OpenMP)"),
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -337,6 +357,7 @@ def run_ours(a, rank, world, local_rank):
     kern = KERNEL_OF_FIELD[a.field]
     kl, kms, kwork = M.profile_read(kern)
     rl, rms, _ = M.profile_read("remesh")
+    sim.close()
     t_max = total_ms
     if dist:
         t_max, (pairs, evals) = combine_ranks(total_ms, [pairs, evals])
@@ -349,21 +370,153 @@ def run_ours(a, rank, world, local_rank):
                "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if a.field.endswith("32c") else "f64",
                "data": "synthetic (deck-generated, no dataset)",
-               "config": {"workload": name, "points": n, "field": a.field, "eps": deck["greens_epsilon"],
-                          "dt": deck["dt"], "remesh_period": deck["remesh_period"], "parallelism": f"replicas{world}",
-                          "l2": "flushed (256 MiB write) between timed steps"},
+               "config": workload_config(name, deck, n, world),
+               "field": a.field, "l2": "flushed (256 MiB write) between timed steps",
+               "value_note": VALUE_NOTE.get(a.field, ""),
                "rk4_steps_per_s": a.steps / (t_max / 1e3) * world,
                "kernel_evals_per_s": evals / (t_max / 1e3),
                "remesh_ms_per_remesh": (rms / rl) if rl else None,
                "gpu_launches": int(launches),
                "roofline": roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src),
                "clocks": clk.summary()}
+        if not a.no_accuracy:
+            acc = accuracy_vs_fp64(a, deck, local_rank, a.drift_steps or (a.warmup + a.steps), sm, peaks)
+            res["accuracy"] = acc["accuracy"]
+            res["plain_fp64_gpu"] = acc["plain_fp64_gpu"]
+            res["speedup_vs_plain_fp64_gpu"] = value / acc["plain_fp64_gpu"]["value"]
+        if not a.no_batch and a.workload == "two_stream":
+            res["batch"] = batch_summary(local_rank, a.batch, 2, 4)
         if not a.no_e2e:
-            res["e2e"] = e2e_plugin(deck, a.field, n, local_rank)
+            res["e2e"] = e2e_plugin(deck, a.field, n, local_rank, a.steps)
         if not a.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(deck, a.cpu_seconds, a.field.startswith("treecode"))
-    sim.close()
     return res
+
+
+VALUE_NOTE = {
+    "direct32c": "pairs are direct-equivalent: N^2 per full evaluation (and U^2 per reduced-grid evaluation) at the "
+                 "accuracy stated in `accuracy`; far pairs (|d| > 16 eps) are summed as an exact FP64 sign part plus a "
+                 "one-term series of analytic error <= v^2/16 (v = eps^2/(d^2+eps^2)), band pairs exactly in FP32 with "
+                 "compensation",
+    "direct64": "pairs evaluated one by one with the reference's FP64 arithmetic (bit-identical)",
+    "treecode32c": "pairs are direct-equivalent N^2 per evaluation; the treecode evaluates near-field pairs and "
+                   "far-field cluster terms (kernel_evals_per_s)",
+    "treecode64": "pairs are direct-equivalent N^2 per evaluation; the treecode evaluates near-field pairs and "
+                  "far-field cluster terms (kernel_evals_per_s)",
+}
+
+# FP64 pipe: 64 FP64 lanes per clock per SM on B200 (half the FP32 lanes).
+FP64_LANES_PER_CLK_PER_SM = 64
+# FP64-pipe thread instructions per pair of k_direct64 (DFMA + DADD + DMUL +
+# DSETP and the other FP64-pipe operations of its two IEEE divisions, square
+# root, round and compares), counted by ncu on the two-stream workload; None
+# until counted.
+DIRECT64_FP64_INSTR_PER_PAIR = None
+
+
+def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):
+    """FP32c against the plain FP64 path on the same workload, from t = 0:
+
+    * field_energy_drift = max_t |W32(t) - W64(t)| / max_t W64(t) over `steps`
+      steps of an FP32c session and an FP64 session (W = 1/2 sum dx E^2 at the
+      unique x in [0, L), the reference's diagnostic);
+    * e_rel_l2 = ||E32 - E64|| / ||E64|| of one field evaluation of each kind
+      on the FP32c session's final state (all N targets and sources);
+    * plain_fp64_gpu: pair-interactions/s of the FP64 session (k_direct64, the
+      reference arithmetic bit for bit; k_far_near64 for the treecode), CUDA
+      events, with its kernel's FP64-pipe fraction."""
+    import multi_species_b200 as M
+    L = deck["xmax"] - deck["xmin"]
+    tree = a.field.startswith("treecode")
+    k64 = "treecode64" if tree else "direct64"
+    s32 = M.Simulation(deck, field_backend=a.field, device=local_rank)
+    s64 = M.Simulation(deck, field_backend=k64, device=local_rank)
+    w32, w64 = [M.field_energy(s32.state()["xs"], s32.state()["es"], L)], []
+    w64.append(M.field_energy(s64.state()["xs"], s64.state()["es"], L))
+    M.profile_reset()
+    M.profile_enable(True)
+    t64, p64 = 0.0, 0.0
+    for _ in range(steps):
+        s32.step(1)
+        q0, _ = s64.work()
+        s64.step(1)
+        t64 += float(np.sum(s64.step_times()))
+        p64 += s64.work()[0] - q0
+        st32, st64 = s32.state(), s64.state()
+        w32.append(M.field_energy(st32["xs"], st32["es"], L))
+        w64.append(M.field_energy(st64["xs"], st64["es"], L))
+    M.profile_enable(False)
+    kern64 = KERNEL_OF_FIELD[k64]
+    kl, kms, kwork = M.profile_read(kern64)
+    s32.close()
+    s64.close()
+    w32, w64 = np.array(w32), np.array(w64)
+    if tree:
+        f32 = M.E_MQ_Treecode_B200(L, deck["greens_epsilon"], deck["mac"], deck["degree"], deck["max_source"],
+                                   precision="fp32c", device=local_rank)
+        f64 = M.E_MQ_Treecode_B200(L, deck["greens_epsilon"], deck["mac"], deck["degree"], deck["max_source"],
+                                   precision="fp64", device=local_rank)
+    else:
+        f32 = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], "fp32c", device=local_rank)
+        f64 = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], "fp64", device=local_rank)
+    x, q = st32["xs"], st32["q_ws"]
+    e32, e64 = f32.evaluate(x, x, q), f64.evaluate(x, x, q)
+    f32.close()
+    f64.close()
+    acc = {"e_rel_l2": float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64)),
+           "e_reference": f"{k64} on the same state (all {len(x)} targets)",
+           "field_energy_drift": float(np.max(np.abs(w32 - w64)) / np.max(w64)),
+           "drift_steps": steps,
+           "target": "e_rel_l2 <= 1e-6, field_energy_drift <= 1e-5"}
+    mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    plain = {"value": p64 / (t64 / 1e3), "unit": "pair-interactions/s", "path": f"{k64} Simulation, same deck",
+             "steps": steps, "ms_per_step": t64 / steps}
+    if not tree and kms > 0 and DIRECT64_FP64_INSTR_PER_PAIR:
+        rate = kwork / (kms / 1e3)
+        peak = sm * FP64_LANES_PER_CLK_PER_SM * mhz * 1e6 / DIRECT64_FP64_INSTR_PER_PAIR
+        plain["roofline"] = {"kernel": kern64, "bound": "fp64-pipe", "unit": "Gpair/s", "achieved": rate / 1e9,
+                             "peak": peak / 1e9, "frac": rate / peak,
+                             "peak_source": f"{sm} SMs x {FP64_LANES_PER_CLK_PER_SM} FP64 lanes/clk x {mhz:.0f} MHz / "
+                                            f"{DIRECT64_FP64_INSTR_PER_PAIR} FP64-pipe instructions per pair "
+                                            "(ncu count, profiles/k_direct64_two_stream.md)"}
+    return {"accuracy": acc, "plain_fp64_gpu": plain}
+
+
+def batch_summary(local_rank, count, warmup, steps):
+    """Compact C4 record: `count` seeded Landau instances stepped together
+    (one persistent pair launch per field evaluation, autotuned, graph-replayed
+    steps), p50/p99 step latency and the rate against the plain FP64 path on
+    the batch's largest instance."""
+    import multi_species_b200 as M
+    from multi_species_b200 import decks
+    ds = decks.landau_batch(count=count, seed=0)
+    b = M.Batch(device=local_rank)
+    for d in ds:
+        b.add(d)
+    b.step(warmup)
+    p0 = b.pair_count()
+    ms = []
+    for _ in range(steps):
+        b.step(1)
+        ms.extend(b.step_times().tolist())
+    pairs = b.pair_count() - p0
+    st = b.stats()
+    b.close()
+    big = max(ds, key=decks.deck_points)
+    sim = M.Simulation(big, field_backend="direct64", device=local_rank)
+    sim.step(1)
+    w0, _ = sim.work()
+    sim.step(1)
+    plain = (sim.work()[0] - w0) / (float(np.sum(sim.step_times())) / 1e3)
+    sim.close()
+    value = pairs / (float(np.sum(ms)) / 1e3)
+    return {"workload": f"landau_batch{count}", "instances": len(ds),
+            "points_total": int(sum(decks.deck_points(d) for d in ds)), "steps": steps, "warmup": warmup,
+            "value": value, "unit": "pair-interactions/s", "step_ms_p50": float(np.percentile(ms, 50)),
+            "step_ms_p99": float(np.percentile(ms, 99)), "plain_fp64_gpu": plain,
+            "speedup_vs_plain_fp64_gpu": value / plain,
+            "tuning": {k: st[k] for k in ("targets_per_thread", "tiles_per_item")},
+            "graph_steps": st["graph_steps"]}
 
 
 def run_batch(a, rank, world, local_rank):
@@ -433,11 +586,11 @@ def run_batch(a, rank, world, local_rank):
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (deck-generated, no dataset)",
            "config": {"workload": f"landau_batch{a.batch}", "instances": len(ds), "points_total": int(sum(npts)),
-                      "points_min": int(min(npts)), "points_max": int(max(npts)), "field": "direct32c",
-                      "eps": 0.05, "dt": 0.25, "remesh_period": 5, "parallelism": f"replicas{world}",
-                      "l2": "flushed (256 MiB write) between timed steps",
-                      "tuning": {k: stats[k] for k in ("targets_per_thread", "tiles_per_item")},
-                      "graph_steps": stats["graph_steps"], "plain_steps": stats["plain_steps"]},
+                      "points_min": int(min(npts)), "points_max": int(max(npts)),
+                      "eps": 0.05, "dt": 0.25, "remesh_period": 5, "parallelism": f"replicas{world}"},
+           "field": "direct32c", "l2": "flushed (256 MiB write) between timed steps",
+           "tuning": {k: stats[k] for k in ("targets_per_thread", "tiles_per_item")},
+           "graph_steps": stats["graph_steps"], "plain_steps": stats["plain_steps"],
            "rk4_steps_per_s": a.steps * len(ds) / (t_max / 1e3) * world,
            "plain_fp64_gpu": {"value": plain, "unit": "pair-interactions/s",
                               "path": "direct64 Simulation (reference arithmetic), largest instance alone",
@@ -447,7 +600,7 @@ def run_batch(a, rank, world, local_rank):
            "ms_per_step_by_phase": breakdown,
            "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
     if not a.no_e2e:
-        res["e2e"] = e2e_plugin(big, "direct32c", decks.deck_points(big), local_rank)
+        res["e2e"] = e2e_plugin(big, "direct32c", decks.deck_points(big), local_rank, a.steps)
         res["e2e"]["note"] = "plugin path on the batch's largest instance"
     if not a.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline(big, a.cpu_seconds, False)
@@ -576,7 +729,13 @@ def host_rk4_step(field, xs, ps, es, qw, qm, dt, work=None):
     return xs, ps, es
 
 
-def e2e_plugin(deck, field_kind, n, device):
+def e2e_plugin(deck, field_kind, n, device, steps=2):
+    """The metric through the reference-facing plugin call with HOST arrays:
+    E_MQ_DirectSum_B200 / E_MQ_Treecode_B200 (es, targets, nt, sources, q_ws, ns)
+    driving the caller's host RK4 step, `steps` steps after one warm-up step.
+    Bytes are counted from the arrays each call hands over: sources and
+    weights host->device (targets too when they are a different array) and E
+    device->host."""
     import multi_species_b200 as M
     sim = M.Simulation(deck, field_backend=field_kind, device=device)
     st = sim.state()
@@ -592,24 +751,27 @@ def e2e_plugin(deck, field_kind, n, device):
     qm = np.concatenate([np.full(c, sp["q"] / sp["m"]) for c, sp in zip(counts, deck["species_list"])])
     xs, ps, es, qw = st["xs"], st["ps"], st["es"], st["q_ws"]
     in_calls = [0.0]
+    moved = [0, 0]
 
-    def timed_field(*args):
+    def timed_field(es_, targets, nt, sources, q_ws, ns):
         c0 = time.perf_counter()
-        f(*args)
+        f(es_, targets, nt, sources, q_ws, ns)
         in_calls[0] += time.perf_counter() - c0
+        moved[0] += sources[:ns].nbytes + q_ws[:ns].nbytes + (0 if targets is sources else targets[:nt].nbytes)
+        moved[1] += es_[:nt].nbytes
 
     work = [np.empty(len(xs)) for _ in range(9)]
     xs, ps, es = host_rk4_step(timed_field, xs, ps, es, qw, qm, deck["dt"], work)  # warm-up
-    steps = 2
     in_calls[0] = 0.0
+    moved[0] = moved[1] = 0
     t0 = time.perf_counter()
     for _ in range(steps):
         xs, ps, es = host_rk4_step(timed_field, xs, ps, es, qw, qm, deck["dt"], work)
     dt = time.perf_counter() - t0
     f.close()
     pairs = 4.0 * n * n * steps
-    return {"value": pairs / dt, "unit": "pair-interactions/s", "h2d_bytes_per_step": 4 * 16 * n,
-            "d2h_bytes_per_step": 4 * 8 * n, "steps": steps,
+    return {"value": pairs / dt, "unit": "pair-interactions/s", "h2d_bytes_per_step": moved[0] / steps,
+            "d2h_bytes_per_step": moved[1] / steps, "steps": steps,
             "ms_per_plugin_call": 1e3 * in_calls[0] / (4 * steps),
             "host_rk4_ms_per_step": 1e3 * (dt - in_calls[0]) / steps,
             "path": f"{type(f).__name__}(es, targets, nt, sources, q_ws, ns) with host arrays, host RK4"}

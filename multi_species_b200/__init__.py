@@ -655,3 +655,20 @@ def mesh(initial_height, p_height, xmin, xmax, pmin, pmax, q=-1.0, quadrature=0)
     _check(lib().fs_mesh_fill(initial_height, p_height, xmin, xmax, pmin, pmax, q, quadrature, _ptr(xs), _ptr(ps),
                               panels.ctypes.data_as(_ip), leaves.ctypes.data_as(_ip), _ptr(w)))
     return {"xs": xs, "ps": ps, "panels": panels, "leaves": leaves, "base_weights": w}
+
+
+def field_energy(xs, es, L: float) -> float:
+    """Electrostatic field energy W = 1/2 sum dx E^2 of a state, the potential
+    energy of the reference's diagnostics (standard_interface/diagnostic_plot.py:122-130):
+    E at the unique positions inside [0, L), each weighted by half the distance
+    between its periodic neighbours.  Host arithmetic on exported arrays."""
+    xs = np.asarray(xs, dtype=np.float64)
+    es = np.asarray(es, dtype=np.float64)
+    x_sort, idx = np.unique(xs, return_index=True)
+    e_sort = es[idx]
+    keep = np.nonzero((x_sort >= 0) * (x_sort < L))
+    mx, me = x_sort[keep], e_sort[keep]
+    dxs = 0.5 * np.hstack([mx[1] + L - mx[-1], mx[2:] - mx[:-2], mx[0] + L - mx[-2]])
+    if np.any(dxs <= 0):
+        raise ValueError("field_energy: positions need at least three distinct values in [0, L)")
+    return 0.5 * float(np.dot(dxs, me ** 2))

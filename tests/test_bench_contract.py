@@ -50,3 +50,27 @@ def test_reference_arm_under_two_ranks():
     assert len(lines) == 1
     _check_line(lines[0])
     assert lines[0]["n_gpus"] == 2
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm times the reference alone: the product's CUDA library
+    is never mapped into its process."""
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', "
+            "'--cpu-seconds', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_MAPPED' if 'libfs_b200' in maps else 'PRODUCT_NOT_MAPPED')")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "PRODUCT_NOT_MAPPED" in r.stdout
+
+
+def test_reference_arm_config_is_the_workload_config():
+    """Both arms describe the workload with the same config dict."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from multi_species_b200 import decks
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                        "--cpu-seconds", "1"], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    line = _json_lines(r.stdout)[0]
+    d = decks.two_stream(h=8, ph=1, steps=100, remesh_period=5)
+    assert line["config"] == bench.workload_config("two_stream_precision_form", d, decks.deck_points(d), 1)
