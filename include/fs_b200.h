@@ -69,7 +69,8 @@ fs_status fs_field_create(const fs_field_params* params, fs_field** out);
 fs_status fs_field_destroy(fs_field* field);
 
 /* ElectricField::operator() drop-in (inc/FieldStructure.hpp:87-93): host
- * arrays, synchronous.  Fully overwrites es[0..nt).  For the treecode kinds the
+ * arrays, synchronous.  Fully overwrites es[0..nt) (undefined when the call
+ * returns an error).  For the treecode kinds the
  * reference ignores targets/nt and writes es[0..ns); so does this call
  * (nt must equal ns). */
 fs_status fs_field_eval(fs_field* field, double* es, const double* targets, int nt,
@@ -93,9 +94,23 @@ fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_ta
  * n is limited to 32768 (larger n returns FS_ERR_ARG).  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) for that
  * device; make that first call before any stream capture.  Calls share the
- * array, so calls that overlap on one GPU race: serialise them. */
+ * array, so calls that overlap on one GPU race: serialise them.  The looked-up
+ * address is kept for the life of the process; after cudaDeviceReset on a
+ * device, reload the library before calling this again there.  When the call
+ * returns an error, d_es[0..n) is undefined. */
 fs_status fs_field_eval_noalloc(double L, double epsilon, double* d_es, const double* d_x,
                                 const double* d_q_ws, int n, void* stream);
+
+/* Test hook for the failure paths (no counterpart in the reference): the
+ * bounds of the library's device waits on `device`.  mbar_polls is how many
+ * times a pair kernel polls for a source tile before it reports
+ * FS_ERR_TIMEOUT (0 = give up at once; < 0 = the default bound); walk_panels is
+ * how many panels a remesh point-location walk may visit before it reports
+ * FS_ERR_WALK (<= 0 = the default, 1024).  The bounds are per device and apply
+ * to every later launch until changed.  A call that fails this way leaves its
+ * outputs undefined; the field object or session itself stays usable (a failed
+ * remesh leaves the state it started from). */
+fs_status fs_debug_set_wait_limits(int device, long long mbar_polls, int walk_panels);
 
 /* ------------------------------------------------------------------ session */
 /* One species of the deck (AMRSimulation_load.cpp:188-270 keys). */

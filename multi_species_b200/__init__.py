@@ -45,7 +45,7 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
            "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
            "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes", "fs_sim_set_output",
-           "fs_sim_flush_output", "fs_sim_restart", "fs_initial_f0"]
+           "fs_sim_flush_output", "fs_sim_restart", "fs_initial_f0", "fs_debug_set_wait_limits"]
 
 
 class FsError(RuntimeError):
@@ -116,6 +116,7 @@ def lib():
                                            C.c_int, C.c_void_p]
         L.fs_field_eval_noalloc.argtypes = [C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                             C.c_void_p]
+        L.fs_debug_set_wait_limits.argtypes = [C.c_int, C.c_longlong, C.c_int]
         L.fs_sim_create.argtypes = [C.POINTER(SimParams), C.POINTER(C.c_void_p)]
         L.fs_sim_destroy.argtypes = [C.c_void_p]
         L.fs_sim_step.argtypes = [C.c_void_p, C.c_int]
@@ -290,6 +291,14 @@ class E_MQ_Treecode_B200(_Field):
                  device=0):
         kind = {"fp64": FS_FIELD_TREECODE64, "fp32c": FS_FIELD_TREECODE32C}[precision]
         super().__init__(L, epsilon, kind, mac, degree, max_source, max_target, device=device)
+
+
+def debug_set_wait_limits(device: int = 0, mbar_polls: int = -1, walk_panels: int = 0) -> None:
+    """Test hook: bounds of the device waits on `device` (fs_debug_set_wait_limits).
+    mbar_polls: polls of a pair kernel's tile wait before FS_ERR_TIMEOUT (0 = at
+    once, < 0 = default); walk_panels: panels a remesh walk may visit before
+    FS_ERR_WALK (<= 0 = default).  Call with no limits to restore the defaults."""
+    _check(lib().fs_debug_set_wait_limits(int(device), int(mbar_polls), int(walk_panels)))
 
 
 def field_eval_noalloc(L, epsilon, d_es, d_x, d_q_ws, n, stream=None):

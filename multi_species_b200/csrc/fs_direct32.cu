@@ -89,8 +89,16 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (long long it = 0; it < (1LL << 22); ++it)
+// Polls of one bounded mbarrier wait before it gives up (each poll may itself
+// suspend the thread for a short, hardware-chosen time).
+constexpr long long kMbarPolls = 1LL << 22;
+// The bound the pair kernels use for the waits on their source tiles.
+// fs_debug_set_wait_limits lowers it (0 = give up at once) so that tests can
+// drive the timeout path; the drain waits of that path always use kMbarPolls.
+__device__ long long g_mbar_polls = kMbarPolls;
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long polls) {
+    for (long long it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -213,6 +221,12 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 #define FS_PAIR_BAND 16.0
 #endif
 constexpr double kBand = FS_PAIR_BAND;  // near band half-width in units of eps
+// Far tiles: bit k set = the k-th source of each eight-source body uses one
+// reciprocal per four targets instead of one per two (see the far loop).
+#ifndef FS_QUAD_MASK
+#define FS_QUAD_MASK 0x00
+#endif
+constexpr unsigned kQuadMask = FS_QUAD_MASK;
 constexpr int kMaxChunks = 64;
 
 // One (target block, source chunk) of a job: kR targets per thread, the
@@ -244,6 +258,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
         acc64[r] = 0.0;
     }
     constexpr uint32_t kBytes = kS * sizeof(float4);
+    const long long polls = g_mbar_polls;
     if (tid == 0) {
         fence_proxy_async();
         mbar_expect_tx(&bar[gk & 1], kBytes);
@@ -256,12 +271,16 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             mbar_expect_tx(&bar[b ^ 1], kBytes);
             bulk_load(buf[b ^ 1], Jb.src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
         }
-        const bool ok = mbar_wait_bounded(&bar[b], (gk >> 1) & 1);
+        const bool ok = mbar_wait_bounded(&bar[b], (gk >> 1) & 1, polls);
         if (!__syncthreads_and(ok)) {
             if (tid == 0) {
                 atomicExch(err, (int)FS_ERR_TIMEOUT);
-                // let a copy still in flight land before the CTA's shared memory is released
-                if (t + 1 < t1) (void)mbar_wait_bounded(&bar[b ^ 1], ((gk + 1) >> 1) & 1);
+                // Both copies this CTA issued may still be in flight: the one
+                // into buf[b] whose wait gave up, and the prefetch into
+                // buf[b ^ 1].  Shared memory is released when the CTA exits,
+                // so let both land first (bounded waits).
+                (void)mbar_wait_bounded(&bar[b], (gk >> 1) & 1, kMbarPolls);
+                if (t + 1 < t1) (void)mbar_wait_bounded(&bar[b ^ 1], ((gk + 1) >> 1) & 1, kMbarPolls);
             }
             return false;
         }
@@ -341,23 +360,55 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
                 acc2[h] = make_float2(0.f, 0.f);
             }
-            // eight sources per unrolled body: 32 independent reciprocal
-            // chains per thread keep MUFU and the FP32 pipe fed together
-            // (unroll 4 measured 3.5% slower, 16 no faster)
-#pragma unroll 8
-            for (int j = 0; j < kS; ++j) {
-                const float4 e = tile[j];
-                const float2 sx2 = make_float2(e.x, e.x);
+            // Eight sources per unrolled body (unroll 4 measured 3.5% slower,
+            // 16 no faster).  Each group of four targets uses, per source
+            // position k of the body, either two pair reciprocals (bit k of
+            // kQuadMask clear) or one quad reciprocal (bit set):
+            //   pair: 8 FP32 lane-ops and 1 MUFU.RCP per 2 pairs (4 lane-ops
+            //         and 0.5 MUFU per pair), which load the FMA
+            //         pipe and MUFU equally;
+            //   quad: 18 lane-ops and 1 MUFU.RCP per 4 pairs (4.5 and 0.25 per
+            //         pair), which moves work from MUFU to the FMA pipe.
+            // Mixing the two lets one pipe bound the loop with slack on the other.
+#pragma unroll 1
+            for (int j0 = 0; j0 < kS; j0 += 8) {
 #pragma unroll
-                for (int h = 0; h < kR / 2; ++h) {
-                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
-                    const float2 r2 = __ffma2_rn(d, d, e2v);
-                    // q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b): one
-                    // reciprocal and one scalar product serve both targets, and
-                    // (qW r_a, qW r_b) are the terms of targets 2h+1 and 2h, so
-                    // acc2[h].x accumulates target 2h+1 and .y target 2h
-                    const float qW = e.z * rcp_approx(r2.x * r2.y);
-                    acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
+                for (int k = 0; k < 8; ++k) {
+                    const float4 e = tile[j0 + k];
+                    const float2 sx2 = make_float2(e.x, e.x);
+#pragma unroll
+                    for (int g = 0; g < kR / 4; ++g) {
+                        const int h0 = 2 * g, h1 = 2 * g + 1;
+                        const float2 d0 = __ffma2_rn(sx2, m1, tau2[h0]);  // tau - s, exact product by -1
+                        const float2 d1 = __ffma2_rn(sx2, m1, tau2[h1]);
+                        const float2 r0 = __ffma2_rn(d0, d0, e2v);
+                        const float2 r1 = __ffma2_rn(d1, d1, e2v);
+                        if ((kQuadMask >> k) & 1) {
+                            // q/2 a1 / r_a = (q/2 a1 W) r_b r_c r_d with
+                            // W = 1/(r_a r_b r_c r_d): one reciprocal for four targets
+                            const float pab = r0.x * r0.y, pcd = r1.x * r1.y;
+                            const float qW = e.z * rcp_approx(pab * pcd);
+                            const float wab = qW * pcd, wcd = qW * pab;
+                            acc2[h0] = __ffma2_rn(r0, make_float2(wab, wab), acc2[h0]);
+                            acc2[h1] = __ffma2_rn(r1, make_float2(wcd, wcd), acc2[h1]);
+                        } else {
+                            // q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b): one
+                            // reciprocal and one scalar product serve both targets
+                            const float qW0 = e.z * rcp_approx(r0.x * r0.y);
+                            const float qW1 = e.z * rcp_approx(r1.x * r1.y);
+                            acc2[h0] = __ffma2_rn(r0, make_float2(qW0, qW0), acc2[h0]);
+                            acc2[h1] = __ffma2_rn(r1, make_float2(qW1, qW1), acc2[h1]);
+                        }
+                        // (w r_a, w r_b) are the terms of targets 2h+1 and 2h:
+                        // acc2[h].x accumulates target 2h+1 and .y target 2h
+                    }
+#pragma unroll
+                    for (int h = 2 * (kR / 4); h < kR / 2; ++h) {  // a last pair of targets (kR = 2)
+                        const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
+                        const float2 r2 = __ffma2_rn(d, d, e2v);
+                        const float qW = e.z * rcp_approx(r2.x * r2.y);
+                        acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
+                    }
                 }
             }
 #pragma unroll
@@ -729,6 +780,11 @@ FieldEngine* make_direct32c(double L, double eps) { return new Direct32c(L, eps)
 // timeout flag is cleared at the start of each call.  Calls whose work overlaps
 // on the same GPU (different streams or threads) race on the array; serialise
 // them.
+void set_mbar_polls(long long polls) {
+    const long long v = polls < 0 ? kMbarPolls : polls;
+    FS_CUDA(cudaMemcpyToSymbol(g_mbar_polls, &v, sizeof(v)));
+}
+
 constexpr int kNoAllocMaxPoints = 32768;
 constexpr int kNoAllocMaxChunks = 16;
 constexpr size_t kNoAllocCubBytes = size_t(2) << 20;

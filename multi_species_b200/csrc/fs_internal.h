@@ -249,6 +249,10 @@ int pairs_batched_grid(int R);
 // work of each (tiles x targets), appended to `items` / `cost`.
 void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost);
 
+// Polls of the pair kernels' tile waits on the current device (< 0: the
+// default bound); a test hook behind fs_debug_set_wait_limits.
+void set_mbar_polls(long long polls);
+
 FieldEngine* make_direct64(double L, double eps);
 FieldEngine* make_direct64_open(double eps);
 FieldEngine* make_direct32c(double L, double eps);

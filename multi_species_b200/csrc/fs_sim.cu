@@ -57,6 +57,9 @@ constexpr int kT = 256;
 // does); a walk longer than kHist panels stops with FS_ERR_WALK instead of
 // forgetting where it has been.
 constexpr int kHist = 1024;
+// Walk length at which a walk gives up (<= kHist); fs_debug_set_wait_limits
+// lowers it so that tests can drive FS_ERR_WALK.
+__device__ int g_walk_limit = kHist;
 
 __device__ __forceinline__ void raise_status(int* status, int code) { atomicCAS(status, 0, code); }
 
@@ -184,6 +187,7 @@ __device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const
                          double& tx, double tp, int leaf, bool& beyond, int* __restrict__ hist) {
     const double Lx = M.Lx;
     const int* R = M.rec;
+    const int limit = g_walk_limit;
     int nh = 0;
     hist[nh++] = leaf;
     for (;;) {
@@ -222,7 +226,7 @@ __device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const
         bool seen = false;
         for (int h = 0; h < nh; ++h) seen |= (hist[h] == nl);
         if (seen) return nl;
-        if (nh == kHist) return -1;
+        if (nh >= limit) return -1;
         hist[nh++] = nl;
         leaf = nl;
     }
@@ -522,11 +526,15 @@ __global__ void k_interp_points(MeshView M, const double* __restrict__ ox, const
     fout[k] = v;
 }
 
+// The new state of a remeshed species.  Skipped when an earlier kernel of the
+// remesh reported a failure (status set), so that a failed remesh leaves the
+// state it started from.
 __global__ void k_reset_points(int n, const double* __restrict__ lat_x, const double* __restrict__ lat_p,
                                const double* __restrict__ w0, const double* __restrict__ fnew, double* __restrict__ x,
-                               double* __restrict__ p, double* __restrict__ f, double* __restrict__ qw) {
+                               double* __restrict__ p, double* __restrict__ f, double* __restrict__ qw,
+                               const int* __restrict__ status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= n || *status) return;
     x[k] = lat_x[k];
     p[k] = lat_p[k];
     f[k] = fnew[k];
@@ -543,10 +551,12 @@ __global__ void k_column_sums(int nu, const int* __restrict__ off, const int* __
     rw[u] = s;
 }
 
+// E of every point from the reduced grid; skipped, like k_reset_points, after
+// a failure earlier in the same remesh.
 __global__ void k_scatter_reduced(int n, const int* __restrict__ inv, const double* __restrict__ re,
-                                  double* __restrict__ e) {
+                                  double* __restrict__ e, const int* __restrict__ status) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
+    if (k >= n || *status) return;
     e[k] = re[inv[k]];
 }
 
@@ -1100,7 +1110,7 @@ struct Sim {
     }
     void reduced_post() {
         for (auto& s : sp) {
-            k_scatter_reduced<<<blocks(s->n), kT, 0, st>>>(s->n, s->inv.p, re.p, e.p + s->start);
+            k_scatter_reduced<<<blocks(s->n), kT, 0, st>>>(s->n, s->inv.p, re.p, e.p + s->start, status.p);
         }
         FS_LAUNCHED((long long)sp.size());
     }
@@ -1157,7 +1167,7 @@ struct Sim {
                 any_adaptive = true;  // f at the lattice stays in fnew; the old state is still needed
             } else {
                 k_reset_points<<<blocks(nb), kT, 0, st>>>(nb, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
-                                                         p.p + a, f.p + a, qw.p + a);
+                                                         p.p + a, f.p + a, qw.p + a, status.p);
             }
         }
         FS_LAUNCHED(7LL * (long long)sp.size());
@@ -1461,6 +1471,18 @@ struct fs_sim {
 };
 
 extern "C" {
+
+fs_status fs_debug_set_wait_limits(int device, long long mbar_polls, int walk_panels) {
+    return fsb::guard([&] {
+        int prev = 0;
+        FS_CUDA(cudaGetDevice(&prev));
+        FS_CUDA(cudaSetDevice(device));
+        fsb::set_mbar_polls(mbar_polls);
+        const int w = (walk_panels <= 0 || walk_panels > fsb::kHist) ? fsb::kHist : walk_panels;
+        FS_CUDA(cudaMemcpyToSymbol(fsb::g_walk_limit, &w, sizeof(w)));
+        FS_CUDA(cudaSetDevice(prev));
+    });
+}
 
 fs_status fs_sim_create(const fs_sim_params* params, fs_sim** out) {
     if (!params || !out) return fsb::guard([] { fsb::fail(FS_ERR_ARG, "null argument"); });
