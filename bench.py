@@ -468,6 +468,17 @@ def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):
            "field_energy_drift": float(np.max(np.abs(w32 - w64)) / np.max(w64)),
            "drift_steps": steps,
            "target": "e_rel_l2 <= 1e-6, field_energy_drift <= 1e-5"}
+    if tree:
+        # the treecode's own approximation error, against the plain FP64 direct
+        # sum (rescaled by the treecode kernel's sqrt(L^2 + 4 eps^2) / L) on
+        # 4096 evenly spaced targets
+        idx = np.linspace(0, len(x) - 1, 4096).astype(np.int64)
+        fd = M.E_MQ_DirectSum_B200(L, deck["greens_epsilon"], "fp64", device=local_rank)
+        ed = fd.evaluate(x[idx], x, q) * np.sqrt(L * L + 4 * deck["greens_epsilon"] ** 2) / L
+        fd.close()
+        acc["tree_vs_direct64_sampled"] = {"fp32c": float(np.linalg.norm(e32[idx] - ed) / np.linalg.norm(ed)),
+                                           "fp64": float(np.linalg.norm(e64[idx] - ed) / np.linalg.norm(ed)),
+                                           "targets": len(idx)}
     mhz = float(peaks.get("sm_max_mhz", 1965.0))
     plain = {"value": p64 / (t64 / 1e3), "unit": "pair-interactions/s", "path": f"{k64} Simulation, same deck",
              "steps": steps, "ms_per_step": t64 / steps}

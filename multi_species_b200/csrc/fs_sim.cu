@@ -182,12 +182,13 @@ __device__ __forceinline__ bool edge_bottom(double x_br, double p_br, double x_b
 // step to the neighbour across the first failed edge (right, top, bottom, left
 // priority), shifting tx by Lx across the periodic seam; stop at the first
 // panel already visited.  beyond_boundary is or-ed over every visited panel.
-// Bounded: returns -1 when the walk visits more than kHist panels.
+// Bounded: returns -1 when the walk would visit more than `cap` panels (cap
+// <= the entries of hist).
 __device__ int walk_from(const MeshView& M, const double* __restrict__ ox, const double* __restrict__ op,
-                         double& tx, double tp, int leaf, bool& beyond, int* __restrict__ hist) {
+                         double& tx, double tp, int leaf, bool& beyond, int* __restrict__ hist, int cap) {
     const double Lx = M.Lx;
     const int* R = M.rec;
-    const int limit = g_walk_limit;
+    const int limit = cap;
     int nh = 0;
     hist[nh++] = leaf;
     for (;;) {
@@ -416,7 +417,7 @@ __global__ void k_walk_first_column(MeshView M, int nx, int np, const double* __
         const int pt = ii * nx;
         beyond = false;
         double tx = sortx[pt];
-        leaf = walk_from(M, ox, op, tx, sortp[pt], leaf, beyond, hist);
+        leaf = walk_from(M, ox, op, tx, sortp[pt], leaf, beyond, hist, min(g_walk_limit, kHist));
         if (leaf < 0) {
             raise_status(status, FS_ERR_WALK);
             return;
@@ -440,13 +441,189 @@ __global__ void k_walk_rows(MeshView M, int nx, int np, const double* __restrict
         const int pt = ii * nx + jj;
         bool beyond = false;
         double tx = sortx[pt];
-        lc = walk_from(M, ox, op, tx, sortp[pt], lc, beyond, hist + (size_t)ii * kHist);
+        lc = walk_from(M, ox, op, tx, sortp[pt], lc, beyond, hist + (size_t)ii * kHist, min(g_walk_limit, kHist));
         if (lc < 0) {
             raise_status(status, FS_ERR_WALK);
             return;
         }
         sortx[pt] = tx;
         leaf_of[pt] = beyond ? 0 : lc;
+    }
+}
+
+// ---------------------------------------------------------------- parallel point location
+// The walks above form one chain per lattice row, hung from one chain down the
+// first column: each point's walk starts at the leaf where the previous
+// point's walk ended.  The same result is computed in parallel:
+//   1. a guess of every point's leaf (k_leaf_xmid, k_guess): the leaf of the
+//      old uniform mesh in the point's p-row whose centre is nearest in x;
+//   2. every point's walk at once, each starting at the guess for its
+//      predecessor (k_walk_spec), with a short local history;
+//   3. a warp per chain (k_repair_column, then k_repair_rows) checks in order,
+//      32 points at a time, that each walk started where its predecessor's
+//      final walk ended, and walks again, with the full history, wherever it
+//      did not.  Every final result is then a walk from the final result of
+//      its predecessor: the chain's own result, whatever the guesses were.
+// Used for species whose previous mesh is the uniform lattice mesh (every
+// non-adaptive remesh); adaptive meshes keep the chain kernels above.
+constexpr int kSpecHist = 32;  // local history of a speculative walk
+
+// Centre x of every leaf of the old uniform mesh, by lattice cell (ip, ix).
+__global__ void k_leaf_xmid(int ncell, const int* __restrict__ leaf_grid, const int* __restrict__ rec,
+                            const double* __restrict__ ox, double* __restrict__ xmid) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    xmid[c] = ox[rec[(size_t)leaf_grid[c] * 18 + 4]];
+}
+
+// Guess of the old leaf holding each sorted slot: its p-row by p, then the
+// leaf of that row whose centre is nearest in x, periodically.
+__global__ void k_guess(int n, const double* __restrict__ sortx, const double* __restrict__ sortp, double pmin,
+                        double dpp, int npx, int npp, double Lx, const double* __restrict__ xmid,
+                        const int* __restrict__ leaf_grid, int* __restrict__ guess) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int ip = (int)floor((sortp[k] - pmin) / dpp);
+    ip = min(max(ip, 0), npp - 1);
+    const double* xm = xmid + (size_t)ip * npx;
+    const double x0 = xm[0];
+    double u = sortx[k] - x0;
+    u -= Lx * floor(u / Lx);
+    int lo = 0, hi = npx;  // first ix with xm[ix] - x0 > u
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (xm[mid] - x0 <= u) lo = mid + 1;
+        else hi = mid;
+    }
+    int ix = lo - 1;  // xm[ix] - x0 <= u < xm[ix + 1] - x0
+    if (ix < 0) ix = 0;
+    const double right = (ix + 1 < npx) ? (xm[ix + 1] - x0) : Lx;
+    if (right - u < u - (xm[ix] - x0)) ix = (ix + 1) % npx;
+    guess[k] = leaf_grid[(size_t)ip * npx + ix];
+}
+
+// Every sorted slot's walk from the guess for its predecessor (slot 0: from
+// the root search, as the chain does).  Writes the walk's end leaf R, the
+// start it used S (-2: the walk did not finish within the local history or
+// the walk bound, so the repair walks it again), its beyond-boundary flag B
+// and its x after the periodic shifts TX.
+__global__ void k_walk_spec(MeshView M, int nx, int n, const double* __restrict__ ox, const double* __restrict__ op,
+                            const double* __restrict__ sortx, const double* __restrict__ sortp,
+                            const int* __restrict__ guess, int* __restrict__ wR, int* __restrict__ wS,
+                            int* __restrict__ wB, double* __restrict__ wTX, int* __restrict__ root_leaf,
+                            double* __restrict__ root_x, int* __restrict__ status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double tx = sortx[k];
+    int start;
+    if (k == 0) {
+        bool bb = false;
+        start = find_from_root(M, ox, op, tx, sortp[0], bb);
+        root_leaf[0] = start;
+        root_x[0] = tx;
+        if (start < 0) {
+            raise_status(status, FS_ERR_WALK);
+            wR[0] = 0;
+            wS[0] = -2;
+            wB[0] = 0;
+            wTX[0] = tx;
+            return;
+        }
+    } else {
+        start = (k % nx == 0) ? guess[k - nx] : guess[k - 1];
+    }
+    int hist[kSpecHist];
+    bool beyond = false;
+    const int r = walk_from(M, ox, op, tx, sortp[k], start, beyond, hist, min(kSpecHist, g_walk_limit));
+    wR[k] = r < 0 ? start : r;
+    wS[k] = r < 0 ? -2 : start;
+    wB[k] = beyond ? 1 : 0;
+    wTX[k] = tx;
+}
+
+// One warp walks a chain again where needed.  pos(i) is the slot of the i-th
+// point of the chain (i = 0 .. len-1), start0 the leaf the chain starts from.
+// Returns false after a walk error (status set).
+__device__ bool repair_chain(const MeshView& M, const double* __restrict__ ox, const double* __restrict__ op,
+                             const double* __restrict__ sortx, const double* __restrict__ sortp, int* wR, int* wS,
+                             int* wB, double* wTX, int* __restrict__ hist, int* __restrict__ status, int first_slot,
+                             int stride, int len, int start0, double x0_override, bool use_x0) {
+    const int lane = threadIdx.x & 31;
+    const int cap = min(g_walk_limit, kHist);
+    int i = 0;
+    while (i < len) {
+        const int ii = i + lane;
+        bool bad = false;
+        if (ii < len) {
+            const int k = first_slot + ii * stride;
+            const int want = (ii == 0) ? start0 : wR[k - stride];
+            bad = (wS[k] != want);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, bad);
+        if (!m) {
+            i += 32;
+            continue;
+        }
+        const int f = i + __ffs(m) - 1;
+        int ok = 1;
+        if (lane == 0) {
+            const int k = first_slot + f * stride;
+            const int want = (f == 0) ? start0 : wR[k - stride];
+            double tx = (f == 0 && use_x0) ? x0_override : sortx[k];
+            bool beyond = false;
+            const int r = walk_from(M, ox, op, tx, sortp[k], want, beyond, hist, cap);
+            if (r < 0) {
+                raise_status(status, FS_ERR_WALK);
+                ok = 0;
+            } else {
+                wR[k] = r;
+                wS[k] = want;
+                wB[k] = beyond ? 1 : 0;
+                wTX[k] = tx;
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (!ok) return false;
+        i = f + 1;
+    }
+    return true;
+}
+
+// The first column: one warp.
+__global__ void k_repair_column(MeshView M, int nx, int np, const double* __restrict__ ox,
+                                const double* __restrict__ op, const double* __restrict__ sortx,
+                                const double* __restrict__ sortp, int* wR, int* wS, int* wB, double* wTX,
+                                const int* __restrict__ root_leaf, const double* __restrict__ root_x,
+                                int* __restrict__ hist, int* __restrict__ status) {
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    if (root_leaf[0] < 0) return;  // the root search failed (status set)
+    (void)repair_chain(M, ox, op, sortx, sortp, wR, wS, wB, wTX, hist, status, 0, nx, np, root_leaf[0], root_x[0],
+                       true);
+}
+
+// Every row: one warp per row, then the row's final leaves (0 beyond the
+// p-range) and shifted x.
+__global__ void k_repair_rows(MeshView M, int nx, int np, const double* __restrict__ ox, const double* __restrict__ op,
+                              double* __restrict__ sortx, const double* __restrict__ sortp, int* wR, int* wS, int* wB,
+                              double* wTX, int* __restrict__ leaf_of, int* __restrict__ hist,
+                              int* __restrict__ status) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= np) return;
+    const int lane = threadIdx.x & 31;
+    const int first = row * nx;
+    // the first column failed: one read for the whole warp, so that no lane
+    // leaves while the others enter the warp-wide scan
+    int failed = (lane == 0) ? *(volatile int*)status : 0;
+    failed = __shfl_sync(0xffffffffu, failed, 0);
+    if (failed) return;
+    const bool ok = repair_chain(M, ox, op, sortx, sortp, wR, wS, wB, wTX, hist + (size_t)row * kHist, status,
+                                 first + 1, 1, nx - 1, wR[first], 0.0, false);
+    if (!ok) return;
+    for (int j = lane; j < nx; j += 32) {
+        const int k = first + j;
+        leaf_of[k] = wB[k] ? 0 : wR[k];
+        sortx[k] = wTX[k];
     }
 }
 
@@ -595,6 +772,11 @@ struct SpeciesState {
     DevBuf<double> sx, sortx, sortp;
     DevBuf<int> order, leaf_of, first_col, walk_hist;
     int nxl = 0, npl = 0, pow2 = 1;
+    // parallel point location (uniform previous mesh): leaf of each lattice
+    // cell, leaf centres, guesses and the speculative walks' results
+    bool grid_ok = false;
+    DevBuf<int> leaf_grid, wG, wR, wS, wB, wroot;
+    DevBuf<double> xmid, wTX, wroot_x;
     // reduced grid
     int nu = 0, roff = 0;
     DevBuf<int> inv, col_off, col_idx;
@@ -874,6 +1056,36 @@ struct Sim {
         upload(ss.leaf_slot, slot);
         ss.nleaves = (int)M.leaves.size();
         ss.coef.ensure((size_t)ss.nleaves * 11);
+        // lattice cell of every leaf when the mesh is the uniform npx x npp one
+        // (each leaf covers the 3 x 3 lattice points from (2 ix, 2 ip))
+        ss.grid_ok = false;
+        if (!ss.adaptive && ss.npx > 0 && ss.npp > 0 && (int)M.leaves.size() == ss.npx * ss.npp) {
+            const double hx = (M.xmax - M.xmin) / ss.npx / 2, hp = (M.pmax - M.pmin) / ss.npp / 2;
+            std::vector<int> grid((size_t)ss.npx * ss.npp, -1);
+            bool ok = true;
+            for (int l : M.leaves) {
+                const int* r = &rec[(size_t)l * 18];
+                const double c0 = (M.xs[r[0]] - M.xmin) / hx, r0 = (M.ps[r[0]] - M.pmin) / hp;
+                const double c8 = (M.xs[r[8]] - M.xmin) / hx, r8 = (M.ps[r[8]] - M.pmin) / hp;
+                const long ic = std::lround(c0), ir = std::lround(r0);
+                if (std::fabs(c0 - ic) > 1e-6 || std::fabs(r0 - ir) > 1e-6 || std::fabs(c8 - (ic + 2)) > 1e-6 ||
+                    std::fabs(r8 - (ir + 2)) > 1e-6 || (ic & 1) || (ir & 1)) {
+                    ok = false;
+                    break;
+                }
+                const long ix = ic / 2, ip = ir / 2;
+                if (ix < 0 || ix >= ss.npx || ip < 0 || ip >= ss.npp || grid[(size_t)ip * ss.npx + ix] != -1) {
+                    ok = false;
+                    break;
+                }
+                grid[(size_t)ip * ss.npx + ix] = l;
+            }
+            if (ok) {
+                upload(ss.leaf_grid, grid);
+                ss.xmid.ensure(grid.size());
+                ss.grid_ok = true;
+            }
+        }
     }
 
     // Reduced grid of a species (get_reduced_xs_ws, AMRStructure.cpp:147-185):
@@ -1009,6 +1221,10 @@ struct Sim {
             ss->leaf_of.ensure(ss->nbase);
             ss->first_col.ensure(ss->npl);
             ss->walk_hist.ensure((size_t)ss->npl * kHist);
+            for (DevBuf<int>* b : {&ss->wG, &ss->wR, &ss->wS, &ss->wB}) b->ensure(ss->nbase);
+            ss->wTX.ensure(ss->nbase);
+            ss->wroot.ensure(1);
+            ss->wroot_x.ensure(1);
             ss->fnew.ensure(ss->nbase);
             ss->roff = U;
             const std::vector<double> ux = reduced_maps(*ss, M.xs);
@@ -1143,6 +1359,7 @@ struct Sim {
 
     void remesh_kernels() {
         bool any_adaptive = false;
+        long long launches = 0;
         for (auto& s : sp) {
             const int a = s->start;
             const int nb = s->nbase;
@@ -1156,21 +1373,41 @@ struct Sim {
                 FS_CUDA(cudaFuncSetAttribute(k_row_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_row_sort<<<s->npl, 512, smem, st>>>(s->nxl, s->pow2, s->row_pts.p, s->sx.p, s->lat_p.p, s->sortx.p,
                                                   s->sortp.p, s->order.p);
-            k_walk_first_column<<<1, 32, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
-                                                  s->first_col.p, s->leaf_of.p, s->walk_hist.p, status.p);
-            k_walk_rows<<<blocks(s->npl, 64), 64, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
-                                                           s->sortp.p, s->first_col.p, s->leaf_of.p, s->walk_hist.p,
-                                                           status.p);
+            if (s->grid_ok) {
+                const int ncell = s->npx * s->npp;
+                k_leaf_xmid<<<blocks(ncell), kT, 0, st>>>(ncell, s->leaf_grid.p, s->rec.p, x.p + a, s->xmid.p);
+                k_guess<<<blocks(nb), kT, 0, st>>>(nb, s->sortx.p, s->sortp.p, M.pmin, M.dpp, s->npx, s->npp, L,
+                                                   s->xmid.p, s->leaf_grid.p, s->wG.p);
+                k_walk_spec<<<blocks(nb, 128), 128, 0, st>>>(M, s->nxl, nb, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
+                                                             s->wG.p, s->wR.p, s->wS.p, s->wB.p, s->wTX.p, s->wroot.p,
+                                                             s->wroot_x.p, status.p);
+                k_repair_column<<<1, 32, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
+                                                  s->wR.p, s->wS.p, s->wB.p, s->wTX.p, s->wroot.p, s->wroot_x.p,
+                                                  s->walk_hist.p, status.p);
+                k_repair_rows<<<blocks(s->npl, 4), 128, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
+                                                                 s->sortp.p, s->wR.p, s->wS.p, s->wB.p, s->wTX.p,
+                                                                 s->leaf_of.p, s->walk_hist.p, status.p);
+                launches += 5;
+            } else {
+                k_walk_first_column<<<1, 32, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
+                                                      s->first_col.p, s->leaf_of.p, s->walk_hist.p, status.p);
+                k_walk_rows<<<blocks(s->npl, 64), 64, 0, st>>>(M, s->nxl, s->npl, x.p + a, p.p + a, s->sortx.p,
+                                                               s->sortp.p, s->first_col.p, s->leaf_of.p,
+                                                               s->walk_hist.p, status.p);
+                launches += 2;
+            }
             k_eval_points<<<blocks(nb), kT, 0, st>>>(M, s->sortx.p, s->sortp.p, s->order.p, s->leaf_of.p,
                                                      s->fnew.p);
+            launches += 4;  // fit, shift, row sort, evaluation
             if (s->adaptive) {
                 any_adaptive = true;  // f at the lattice stays in fnew; the old state is still needed
             } else {
                 k_reset_points<<<blocks(nb), kT, 0, st>>>(nb, s->lat_x.p, s->lat_p.p, s->w0.p, s->fnew.p, x.p + a,
                                                          p.p + a, f.p + a, qw.p + a, status.p);
+                launches += 1;
             }
         }
-        FS_LAUNCHED(7LL * (long long)sp.size());
+        FS_LAUNCHED(launches);
         if (any_adaptive) adaptive_remesh();
     }
 
