@@ -90,7 +90,7 @@ fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_ta
  * device memory at call time (a pool or arena that owns the device, hosts that
  * allocate only at start-up, threads where cudaMalloc's device-wide
  * synchronisation is not allowed).  All scratch lives in one static device
- * array of about 9 MiB that each GPU loading the library keeps until exit;
+ * array of about 9.5 MiB that each GPU loading the library keeps until exit;
  * n is limited to 32768 (larger n returns FS_ERR_ARG).  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) for that
  * device; make that first call before any stream capture.  Calls share the

@@ -106,6 +106,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_double((long long)k); }
 
+// 1/sqrt(r) in FP64 for r > 0: the hardware approximation refined by one
+// Newton-Raphson step y (3/2 - r y^2 / 2), which squares its relative error.
+__device__ __forceinline__ double rsqrt_nr64(double r) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
+    const double t = y * y;
+    const double u = fma(-0.5 * r, t, 1.5);
+    return y * u;
+}
+
 // x -> [0, L) and its order-preserving key (non-negative doubles sort as
 // unsigned integers).
 __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint64_t* __restrict__ keys,
@@ -126,12 +136,13 @@ __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint6
 // coefficients, folded into the source's charge once here.
 __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
                                  const double* __restrict__ q, int ns, int ns_pad, double a1, double a2,
-                                 float4* __restrict__ src, double* __restrict__ tbase, double* __restrict__ qs,
-                                 double* __restrict__ qx) {
+                                 float4* __restrict__ src, double2* __restrict__ src64, double* __restrict__ tbase,
+                                 double* __restrict__ qs, double* __restrict__ qx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns_pad) return;
     if (j >= ns) {
         src[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        src64[j] = make_double2(0.0, 0.0);
         return;
     }
     const double xj = key_to_x(skeys[j]);
@@ -140,6 +151,7 @@ __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* 
     const double qj = q[sidx[j]];
     const float qh = (float)(0.5 * qj);
     src[j] = make_float4((float)(xj - base), qh, (float)((double)qh * a1), (float)((double)qh * a2));
+    src64[j] = make_double2(xj, 0.5 * qj);
     qs[j] = qj;
     qx[j] = qj * xj;
 }
@@ -235,7 +247,8 @@ constexpr int kMaxChunks = 64;
 // = (gk >> 1) & 1), so the barriers keep alternating across work items.
 // Returns false when a bounded wait gave up (flag set, CTA must stop).
 template <int kR>
-__device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk, float4 (*buf)[kS], uint64_t* bar,
+__device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk, float4 (*buf)[kS],
+                                           double2 (*buf64)[kS], uint64_t* bar,
                                            uint32_t& gk, int* __restrict__ err) {
     constexpr int kTB = kNT * kR;
     const int tid = threadIdx.x;
@@ -257,19 +270,24 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
         U2[r] = T.U2;
         acc64[r] = 0.0;
     }
+    // each tile: the FP32 records and the FP64 records of the same sources,
+    // two bulk copies completing on one barrier
     constexpr uint32_t kBytes = kS * sizeof(float4);
+    constexpr uint32_t kBytes64 = kS * sizeof(double2);
     const long long polls = g_mbar_polls;
     if (tid == 0) {
         fence_proxy_async();
-        mbar_expect_tx(&bar[gk & 1], kBytes);
+        mbar_expect_tx(&bar[gk & 1], kBytes + kBytes64);
         bulk_load(buf[gk & 1], Jb.src + (size_t)t0 * kS, kBytes, &bar[gk & 1]);
+        bulk_load(buf64[gk & 1], Jb.src64 + (size_t)t0 * kS, kBytes64, &bar[gk & 1]);
     }
     for (int t = t0; t < t1; ++t, ++gk) {
         const int b = gk & 1;
         if (tid == 0 && t + 1 < t1) {
             fence_proxy_async();
-            mbar_expect_tx(&bar[b ^ 1], kBytes);
+            mbar_expect_tx(&bar[b ^ 1], kBytes + kBytes64);
             bulk_load(buf[b ^ 1], Jb.src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
+            bulk_load(buf64[b ^ 1], Jb.src64 + (size_t)(t + 1) * kS, kBytes64, &bar[b ^ 1]);
         }
         const bool ok = mbar_wait_bounded(&bar[b], (gk >> 1) & 1, polls);
         if (!__syncthreads_and(ok)) {
@@ -314,41 +332,22 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
         const float4* tile = buf[b];
         if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband)) {
             // band tiles (every pair of the warp within |d| <= band, one image
-            // per target): q/2 * d * y with y = rsqrt(d^2 + eps^2), two targets
-            // per packed FP32x2 op, Kahan-compensated
-            const float2 e2b = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
-            float2 tau2[kR / 2], acc2[kR / 2], ncmp2[kR / 2];
+            // per target): q/2 * d / sqrt(d^2 + eps^2) in FP64 from the FP64
+            // records.  Band terms are O(q/2) and cancel to the (possibly much
+            // smaller) field, so they need FP64's rounding, not FP32's.
+            const double2* tile64 = buf64[b];
+            const double e2d = Jb.eps2d;
+            double T[kR];
 #pragma unroll
-            for (int h = 0; h < kR / 2; ++h) {
-                tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
-                acc2[h] = make_float2(0.f, 0.f);
-                ncmp2[h] = make_float2(0.f, 0.f);
-            }
-#pragma unroll 4
+            for (int r = 0; r < kR; ++r) T[r] = (jend <= J[r]) ? tl[r] : tl[r] + L;  // the tile's image
+#pragma unroll 2
             for (int j = 0; j < kS; ++j) {
-                const float4 e = tile[j];
-                const float2 sx2 = make_float2(e.x, e.x);
-                const float2 qh = make_float2(e.y, e.y);
+                const double2 e = tile64[j];
 #pragma unroll
-                for (int h = 0; h < kR / 2; ++h) {
-                    // differences as FMAs with -1 (exact products), so no sign
-                    // flips are needed: d = tau - s, then Kahan with the
-                    // negated compensation nc = -c
-                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
-                    const float2 r2 = __ffma2_rn(d, d, e2b);
-                    const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                    const float2 g = __fmul2_rn(d, y);
-                    const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
-                    const float2 sum = __fadd2_rn(acc2[h], v);
-                    const float2 t = __ffma2_rn(acc2[h], m1, sum);
-                    ncmp2[h] = __ffma2_rn(t, m1, v);
-                    acc2[h] = sum;
+                for (int r = 0; r < kR; ++r) {
+                    const double d = T[r] - e.x;
+                    acc64[r] = fma(e.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
                 }
-            }
-#pragma unroll
-            for (int h = 0; h < kR / 2; ++h) {
-                acc64[2 * h] += (double)acc2[h].x + (double)ncmp2[h].x;
-                acc64[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
             }
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
@@ -417,8 +416,11 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
             }
         } else {
-            // near band / image split: per-pair image and band, Kahan sum of
-            // q/2 * d*y (near) or -+ q/2 * c (far)
+            // near band / image split: per-pair image and band; band pairs
+            // q/2 * d / sqrt(d^2 + eps^2) in FP64 (as in band tiles), far
+            // pairs -+ q/2 * c in FP32 with a Kahan sum
+            const double2* tile64 = buf64[b];
+            const double e2d = Jb.eps2d;
             float cmp[kR];
 #pragma unroll
             for (int r = 0; r < kR; ++r) cmp[r] = 0.f;
@@ -429,15 +431,21 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 for (int r = 0; r < kR; ++r) {
                     const bool lo_img = idx < J[r];
                     const int u = lo_img ? idx + ns : idx;
-                    const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
-                    const float y = rsqrt_approx(fmaf(d, d, eps2));
-                    const float z = y * y;
-                    const float c = z * fmaf(z, a2, a1);
-                    const float val = (u < U1[r]) ? -c : ((u >= U2[r]) ? c : d * y);
-                    const float v = fmaf(e.y, val, -cmp[r]);
-                    const float sum = acc[r] + v;
-                    cmp[r] = (sum - acc[r]) - v;
-                    acc[r] = sum;
+                    if (u >= U1[r] && u < U2[r]) {
+                        const double2 e64 = tile64[j];
+                        const double d = (lo_img ? tl[r] : tl[r] + L) - e64.x;
+                        acc64[r] = fma(e64.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
+                    } else {
+                        const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
+                        const float y = rsqrt_approx(fmaf(d, d, eps2));
+                        const float z = y * y;
+                        const float c = z * fmaf(z, a2, a1);
+                        const float val = (u < U1[r]) ? -c : c;
+                        const float v = fmaf(e.y, val, -cmp[r]);
+                        const float sum = acc[r] + v;
+                        cmp[r] = (sum - acc[r]) - v;
+                        acc[r] = sum;
+                    }
                 }
             }
 #pragma unroll
@@ -464,11 +472,12 @@ __device__ __forceinline__ void init_bars(uint64_t* bar) {
 template <int kR>
 __global__ void __launch_bounds__(kNT) k_pairs32(PairJob job, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(128) double2 buf64[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
     if ((int)blockIdx.y * job.tpc >= job.ntiles) return;
     init_bars(bar);
     uint32_t gk = 0;
-    (void)pair_block<kR>(job, blockIdx.x, blockIdx.y, buf, bar, gk, err);
+    (void)pair_block<kR>(job, blockIdx.x, blockIdx.y, buf, buf64, bar, gk, err);
 }
 
 // Many jobs (one per simulation of a batch), persistent: a fixed grid of CTAs
@@ -478,6 +487,7 @@ template <int kR>
 __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items,
                                                          int nitems, int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(128) double2 buf64[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_item;
     init_bars(bar);
@@ -490,7 +500,7 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
         if (item >= nitems) break;
         const int4 it = items[item];
         const PairJob job = jobs[it.x];
-        if (!pair_block<kR>(job, it.y, it.z, buf, bar, gk, err)) return;
+        if (!pair_block<kR>(job, it.y, it.z, buf, buf64, bar, gk, err)) return;
     }
 }
 
@@ -501,6 +511,7 @@ template <int kR>
 __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
                                                             int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
+    __shared__ __align__(128) double2 buf64[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int s_item;
     init_bars(bar);
@@ -511,7 +522,7 @@ __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(Pai
         const int item = s_item;
         __syncthreads();
         if (item >= nitems) break;
-        if (!pair_block<kR>(job, item % tblocks, item / tblocks, buf, bar, gk, err)) return;
+        if (!pair_block<kR>(job, item % tblocks, item / tblocks, buf, buf64, bar, gk, err)) return;
     }
 }
 
@@ -657,7 +668,8 @@ class Direct32c final : public FieldEngine {
             size_t tb = cub_.bytes();
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
             k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
-                                                                 e2 * e2 / 8, src_.p, tbase_.p, qs_.p, qx_.p);
+                                                                 e2 * e2 / 8, src_.p, src64_.p, tbase_.p, qs_.p,
+                                                                 qx_.p);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
             tb = cub_.bytes();
@@ -685,8 +697,8 @@ class Direct32c final : public FieldEngine {
         k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_, pq_.p,
                                                          info_.p);
         FS_LAUNCHED(1);
-        *job = PairJob{src_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
-                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2)};
+        *job = PairJob{src_.p, src64_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
         return true;
     }
 
@@ -708,6 +720,7 @@ class Direct32c final : public FieldEngine {
         iin_.ensure(ns);
         iout_.ensure(ns);
         src_.ensure(ns_pad);
+        src64_.ensure(ns_pad);
         qs_.ensure(ns);
         qx_.ensure(ns);
         pq_.ensure(ns);
@@ -751,6 +764,7 @@ class Direct32c final : public FieldEngine {
     DevBuf<uint64_t> kin_, kout_, tkin_, tkout_;
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
+    DevBuf<double2> src64_;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
@@ -794,7 +808,7 @@ namespace {
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct NoAllocLayout {
-    size_t kin, kout, iin, iout, src, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
+    size_t kin, kout, iin, iout, src, src64, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
 };
 
 constexpr NoAllocLayout noalloc_layout() {
@@ -806,6 +820,7 @@ constexpr NoAllocLayout noalloc_layout() {
     L.iin = o;     o += align256(n * sizeof(int));
     L.iout = o;    o += align256(n * sizeof(int));
     L.src = o;     o += align256(n * sizeof(float4));
+    L.src64 = o;   o += align256(n * sizeof(double2));
     L.tbase = o;   o += align256((n / kS) * sizeof(double));
     L.qs = o;      o += align256(n * sizeof(double));
     L.qx = o;      o += align256(n * sizeof(double));
@@ -869,6 +884,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     int* iin = reinterpret_cast<int*>(at(kNoAlloc.iin));
     int* iout = reinterpret_cast<int*>(at(kNoAlloc.iout));
     float4* src = reinterpret_cast<float4*>(at(kNoAlloc.src));
+    double2* src64 = reinterpret_cast<double2*>(at(kNoAlloc.src64));
     double* tbase = reinterpret_cast<double*>(at(kNoAlloc.tbase));
     double* qs = reinterpret_cast<double*>(at(kNoAlloc.qs));
     double* qx = reinterpret_cast<double*>(at(kNoAlloc.qx));
@@ -903,15 +919,15 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     size_t tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, iin, iout, n, 0, 63, st));
     const double e2 = eps * eps;
-    k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, tbase,
-                                                         qs, qx);
+    k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, src64,
+                                                         tbase, qs, qx);
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
-    const PairJob job{src, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
-                      (float)(e2 * e2 / 8), (float)(0.75 * e2)};
+    const PairJob job{src, src64, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
+                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
     launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;

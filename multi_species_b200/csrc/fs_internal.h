@@ -193,6 +193,7 @@ struct TargetInfo {
 // One field evaluation's FP32 pair work, as the pair kernels see it.
 struct PairJob {
     const float4* src;        // tile-relative source records {s, q/2, q/2 a1, q/2 a2}
+    const double2* src64;     // the same sources in FP64: {x (wrapped), q/2}, for band pairs
     const double* tbase;      // FP64 tile bases
     const TargetInfo* info;   // per sorted target (nt_pad entries)
     double* partial;          // chunks * nt_pad
@@ -200,6 +201,7 @@ struct PairJob {
     double L;
     float eps2, a1, a2;  // near band: eps^2, eps^2/2, eps^4/8
     float e2f;           // far pairs: 3 eps^2 / 4
+    double eps2d;        // band pairs (FP64): eps^2
 };
 
 class FieldEngine {
