@@ -407,11 +407,12 @@ VALUE_NOTE = {
 
 # FP64 pipe: 64 FP64 lanes per clock per SM on B200 (half the FP32 lanes).
 FP64_LANES_PER_CLK_PER_SM = 64
-# FP64-pipe thread instructions per pair of k_direct64 (DFMA + DADD + DMUL +
-# DSETP and the other FP64-pipe operations of its two IEEE divisions, square
-# root, round and compares), counted by ncu on the two-stream workload; None
-# until counted.
-DIRECT64_FP64_INSTR_PER_PAIR = None
+# FP64 thread instructions per pair of k_direct64 (its two IEEE divisions,
+# square root, round, compares and the term: 17.1 DFMA + 12.0 DMUL + 8.0 DADD
+# + 3.1 others), counted by ncu (sm__sass_thread_inst_executed_op_fp64_pred_on
+# over the launch's pairs) on the two-stream deck at 33,153 points; the count
+# per pair does not depend on the size.
+DIRECT64_FP64_INSTR_PER_PAIR = 40.2
 
 
 def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):

@@ -137,7 +137,7 @@ __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint6
 __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
                                  const double* __restrict__ q, int ns, int ns_pad, double a1, double a2,
                                  float4* __restrict__ src, double2* __restrict__ src64, double* __restrict__ tbase,
-                                 double* __restrict__ qs, double* __restrict__ qx) {
+                                 double* __restrict__ qs, double* __restrict__ qx, double* __restrict__ q2) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns_pad) return;
     if (j >= ns) {
@@ -153,6 +153,7 @@ __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* 
     src[j] = make_float4((float)(xj - base), qh, (float)((double)qh * a1), (float)((double)qh * a2));
     src64[j] = make_double2(xj, 0.5 * qj);
     qs[j] = qj;
+    q2[j] = 0.25 * qj * qj;  // (q/2)^2, summed over each target's band by the band-mode estimate
     qx[j] = qj * xj;
 }
 
@@ -220,6 +221,75 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
     info[i] = T;
 }
 
+// Band arithmetic per evaluation.  Summed in FP32, band terms (O(q/2) each)
+// leave an error in E of about kBandKappa * ||S||, S_i^2 = the sum of (q_j/2)^2
+// over target i's band -- they cancel to the field, but their roundings do
+// not.  FP32 band terms are used when that error stays below kBandBudget of the
+// previous field's norm (the field changes little between evaluations), FP64
+// band terms otherwise or when no previous field is known.
+#ifndef FS_BAND_KAPPA
+#define FS_BAND_KAPPA 1.5e-7
+#endif
+constexpr double kBandKappa = FS_BAND_KAPPA;
+constexpr double kBandBudget = 2.5e-7;
+constexpr int kBandStatBlocks = 296;
+
+// Per block: partial sums over targets of S_i^2 and of the previous E_i^2.
+__global__ void __launch_bounds__(256) k_band_stats(int nt, const TargetInfo* __restrict__ info,
+                                                    const double* __restrict__ pq2, int ns,
+                                                    const int* __restrict__ tperm, const double* __restrict__ eref,
+                                                    double* __restrict__ part) {
+    __shared__ double sh[2][256];
+    double s2 = 0.0, e2 = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
+        const TargetInfo T = info[i];
+        s2 += unrolled_prefix(pq2, ns, T.U2) - unrolled_prefix(pq2, ns, T.U1);
+        const double ev = eref[tperm[i]];
+        e2 += ev * ev;
+    }
+    sh[0][threadIdx.x] = s2;
+    sh[1][threadIdx.x] = e2;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = sh[0][0];
+        part[2 * blockIdx.x + 1] = sh[1][0];
+    }
+}
+
+// One block: the sums in a fixed order, the decision, and sqrt(S2 / E2) for
+// diagnostics.
+__global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* __restrict__ part,
+                                                     int* __restrict__ band64, double* __restrict__ ratio) {
+    __shared__ double sh[2][256];
+    double s2 = 0.0, e2 = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+        s2 += part[2 * b];
+        e2 += part[2 * b + 1];
+    }
+    sh[0][threadIdx.x] = s2;
+    sh[1][threadIdx.x] = e2;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double S2 = sh[0][0], E2 = sh[1][0];
+        *band64 = (!(E2 > 0.0) || kBandKappa * kBandKappa * S2 > kBandBudget * kBandBudget * E2) ? 1 : 0;
+        *ratio = E2 > 0.0 ? sqrt(S2 / E2) : -1.0;
+    }
+}
+
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
 // v = eps^2 w, w = 1/(d^2 + eps^2), v <= 1/(1 + kBand^2).  The sign part is
 // summed in FP64 (ffar); the pair kernel accumulates q/2 * c with the shifted
@@ -275,6 +345,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
     constexpr uint32_t kBytes = kS * sizeof(float4);
     constexpr uint32_t kBytes64 = kS * sizeof(double2);
     const long long polls = g_mbar_polls;
+    const bool b64 = *Jb.band64 != 0;  // the job's band arithmetic, decided on the device
     if (tid == 0) {
         fence_proxy_async();
         mbar_expect_tx(&bar[gk & 1], kBytes + kBytes64);
@@ -330,11 +401,11 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             inband &= band;
         }
         const float4* tile = buf[b];
-        if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband)) {
+        if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband) && b64) {
             // band tiles (every pair of the warp within |d| <= band, one image
-            // per target): q/2 * d / sqrt(d^2 + eps^2) in FP64 from the FP64
+            // per target), FP64 mode: q/2 * d / sqrt(d^2 + eps^2) from the FP64
             // records.  Band terms are O(q/2) and cancel to the (possibly much
-            // smaller) field, so they need FP64's rounding, not FP32's.
+            // smaller) field; FP64 keeps their rounding below the field's size.
             const double2* tile64 = buf64[b];
             const double e2d = Jb.eps2d;
             double T[kR];
@@ -348,6 +419,44 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                     const double d = T[r] - e.x;
                     acc64[r] = fma(e.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
                 }
+            }
+        } else if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband)) {
+            // band tiles, FP32 mode (the field is large enough for FP32 band
+            // terms): q/2 * d * y with y = rsqrt(d^2 + eps^2), two targets per
+            // packed FP32x2 op, Kahan-compensated
+            const float2 e2b = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
+            float2 tau2[kR / 2], acc2[kR / 2], ncmp2[kR / 2];
+#pragma unroll
+            for (int h = 0; h < kR / 2; ++h) {
+                tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
+                acc2[h] = make_float2(0.f, 0.f);
+                ncmp2[h] = make_float2(0.f, 0.f);
+            }
+#pragma unroll 4
+            for (int j = 0; j < kS; ++j) {
+                const float4 e = tile[j];
+                const float2 sx2 = make_float2(e.x, e.x);
+                const float2 qh = make_float2(e.y, e.y);
+#pragma unroll
+                for (int h = 0; h < kR / 2; ++h) {
+                    // differences as FMAs with -1 (exact products), so no sign
+                    // flips are needed: d = tau - s, then Kahan with the
+                    // negated compensation nc = -c
+                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
+                    const float2 r2 = __ffma2_rn(d, d, e2b);
+                    const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    const float2 g = __fmul2_rn(d, y);
+                    const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
+                    const float2 sum = __fadd2_rn(acc2[h], v);
+                    const float2 t = __ffma2_rn(acc2[h], m1, sum);
+                    ncmp2[h] = __ffma2_rn(t, m1, v);
+                    acc2[h] = sum;
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < kR / 2; ++h) {
+                acc64[2 * h] += (double)acc2[h].x + (double)ncmp2[h].x;
+                acc64[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
             }
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
@@ -417,8 +526,8 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             }
         } else {
             // near band / image split: per-pair image and band; band pairs
-            // q/2 * d / sqrt(d^2 + eps^2) in FP64 (as in band tiles), far
-            // pairs -+ q/2 * c in FP32 with a Kahan sum
+            // q/2 * d / sqrt(d^2 + eps^2) in FP64 or FP32 (as in band tiles),
+            // far pairs -+ q/2 * c in FP32, FP32 terms with a Kahan sum
             const double2* tile64 = buf64[b];
             const double e2d = Jb.eps2d;
             float cmp[kR];
@@ -431,10 +540,17 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 for (int r = 0; r < kR; ++r) {
                     const bool lo_img = idx < J[r];
                     const int u = lo_img ? idx + ns : idx;
-                    if (u >= U1[r] && u < U2[r]) {
+                    if (u >= U1[r] && u < U2[r] && b64) {
                         const double2 e64 = tile64[j];
                         const double d = (lo_img ? tl[r] : tl[r] + L) - e64.x;
                         acc64[r] = fma(e64.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
+                    } else if (u >= U1[r] && u < U2[r]) {
+                        const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
+                        const float y = rsqrt_approx(fmaf(d, d, eps2));
+                        const float v = fmaf(e.y, d * y, -cmp[r]);
+                        const float sum = acc[r] + v;
+                        cmp[r] = (sum - acc[r]) - v;
+                        acc[r] = sum;
                     } else {
                         const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
                         const float y = rsqrt_approx(fmaf(d, d, eps2));
@@ -624,6 +740,27 @@ class Direct32c final : public FieldEngine {
             const int r = std::atoi(v);
             if (r == 2 || r == 4 || r == 8) R_ = r;
         }
+        // band arithmetic: automatic (default), or forced FP32 ("0") / FP64 ("1")
+        // for measurements of the two
+        if (const char* v = std::getenv("FS_B200_BAND64")) {
+            if (v[0] == '0') band_mode_ = 0;
+            if (v[0] == '1') band_mode_ = 1;
+        }
+    }
+
+    void set_reference_field(const double* e, int n) override {
+        eref_ = e;
+        eref_n_ = n;
+    }
+
+    // sqrt(S2 / E2) of the last automatic band decision (-1: none), for diagnostics
+    double last_band_ratio(cudaStream_t st) {
+        double r = -1.0;
+        if (bandratio_.p) {
+            FS_CUDA(cudaMemcpyAsync(&r, bandratio_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+            FS_CUDA(cudaStreamSynchronize(st));
+        }
+        return r;
     }
 
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
@@ -669,9 +806,11 @@ class Direct32c final : public FieldEngine {
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
             k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
                                                                  e2 * e2 / 8, src_.p, src64_.p, tbase_.p, qs_.p,
-                                                                 qx_.p);
+                                                                 qx_.p, q2_.p);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
+            tb = cub_.bytes();
+            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, q2_.p, pq2_.p, ns, st));
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
             FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
@@ -697,8 +836,16 @@ class Direct32c final : public FieldEngine {
         k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_, pq_.p,
                                                          info_.p);
         FS_LAUNCHED(1);
+        // band arithmetic of this evaluation (a device flag: nothing waits on the host)
+        if (band_mode_ == 2 && eref_ && eref_n_ == nt) {
+            k_band_stats<<<kBandStatBlocks, 256, 0, st>>>(nt, info_.p, pq2_.p, ns, tperm, eref_, bandpart_.p);
+            k_band_decide<<<1, 256, 0, st>>>(kBandStatBlocks, bandpart_.p, band64_.p, bandratio_.p);
+            FS_LAUNCHED(2);
+        } else {
+            FS_CUDA(cudaMemsetAsync(band64_.p, band_mode_ == 0 ? 0 : 1, sizeof(int), st));  // any non-zero byte: FP64
+        }
         *job = PairJob{src_.p, src64_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
-                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, band64_.p};
         return true;
     }
 
@@ -721,6 +868,8 @@ class Direct32c final : public FieldEngine {
         iout_.ensure(ns);
         src_.ensure(ns_pad);
         src64_.ensure(ns_pad);
+        q2_.ensure(ns);
+        pq2_.ensure(ns);
         qs_.ensure(ns);
         qx_.ensure(ns);
         pq_.ensure(ns);
@@ -732,6 +881,10 @@ class Direct32c final : public FieldEngine {
             err_.ensure(1);
             FS_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
             counter_.ensure(1);
+            band64_.ensure(1);
+            bandratio_.ensure(1);
+            bandpart_.ensure(2 * kBandStatBlocks);
+            FS_CUDA(cudaMemset(bandratio_.p, 0, sizeof(double)));
         }
         const int nsort = std::max(ns, nt_sep);
         if (nt_sep) {
@@ -765,6 +918,11 @@ class Direct32c final : public FieldEngine {
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
     DevBuf<double2> src64_;
+    DevBuf<double> q2_, pq2_, bandpart_, bandratio_;
+    DevBuf<int> band64_;
+    int band_mode_ = 2;  // 0 FP32 band, 1 FP64 band, 2 automatic
+    const double* eref_ = nullptr;
+    int eref_n_ = 0;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
@@ -808,7 +966,7 @@ namespace {
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct NoAllocLayout {
-    size_t kin, kout, iin, iout, src, src64, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
+    size_t kin, kout, iin, iout, src, src64, q2, band64, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
 };
 
 constexpr NoAllocLayout noalloc_layout() {
@@ -821,6 +979,8 @@ constexpr NoAllocLayout noalloc_layout() {
     L.iout = o;    o += align256(n * sizeof(int));
     L.src = o;     o += align256(n * sizeof(float4));
     L.src64 = o;   o += align256(n * sizeof(double2));
+    L.q2 = o;      o += align256(n * sizeof(double));
+    L.band64 = o;  o += align256(sizeof(int));
     L.tbase = o;   o += align256((n / kS) * sizeof(double));
     L.qs = o;      o += align256(n * sizeof(double));
     L.qx = o;      o += align256(n * sizeof(double));
@@ -885,6 +1045,8 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     int* iout = reinterpret_cast<int*>(at(kNoAlloc.iout));
     float4* src = reinterpret_cast<float4*>(at(kNoAlloc.src));
     double2* src64 = reinterpret_cast<double2*>(at(kNoAlloc.src64));
+    double* q2 = reinterpret_cast<double*>(at(kNoAlloc.q2));
+    int* band64 = reinterpret_cast<int*>(at(kNoAlloc.band64));
     double* tbase = reinterpret_cast<double*>(at(kNoAlloc.tbase));
     double* qs = reinterpret_cast<double*>(at(kNoAlloc.qs));
     double* qx = reinterpret_cast<double*>(at(kNoAlloc.qx));
@@ -920,14 +1082,15 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, iin, iout, n, 0, 63, st));
     const double e2 = eps * eps;
     k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, src64,
-                                                         tbase, qs, qx);
+                                                         tbase, qs, qx, q2);
+    FS_CUDA(cudaMemsetAsync(band64, 1, sizeof(int), st));  // no previous field here: band pairs in FP64
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
     const PairJob job{src, src64, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
-                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
+                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, band64};
     launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;
