@@ -222,16 +222,18 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 }
 
 // Band arithmetic per evaluation.  Summed in FP32, band terms (O(q/2) each)
-// leave an error in E of about kBandKappa * ||S||, S_i^2 = the sum of (q_j/2)^2
-// over target i's band -- they cancel to the field, but their roundings do
-// not.  FP32 band terms are used when that error stays below kBandBudget of the
-// previous field's norm (the field changes little between evaluations), FP64
-// band terms otherwise or when no previous field is known.
-#ifndef FS_BAND_KAPPA
-#define FS_BAND_KAPPA 1.5e-7
-#endif
-constexpr double kBandKappa = FS_BAND_KAPPA;
-constexpr double kBandBudget = 2.5e-7;
+// leave an error in E of about kappa * ||S||, S_i^2 = the sum of (q_j/2)^2 over
+// target i's band -- the terms cancel to the field, their roundings do not.
+// kappa grows with the tile span in units of eps (the FP32 tile-relative
+// coordinates round in proportion to the span): measured on B200 against the
+// FP64 sum over two-stream, two-species Landau and 2k-66k-point batch decks,
+// kappa <= 6e-8 (1 + 0.15 L / (ntiles eps)) in every case.  FP32 band terms
+// are used when kappa ||S|| stays below kBandBudget times the previous
+// field's norm (the field changes little between evaluations), FP64 band
+// terms otherwise or when no previous field is known.
+constexpr double kBandKappa0 = 6e-8;
+constexpr double kBandSpan = 0.15;
+constexpr double kBandBudget = 4e-7;
 constexpr int kBandStatBlocks = 296;
 
 // Per block: partial sums over targets of S_i^2 and of the previous E_i^2.
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(256) k_band_stats(int nt, const TargetInfo* __
 
 // One block: the sums in a fixed order, the decision, and sqrt(S2 / E2) for
 // diagnostics.
-__global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* __restrict__ part,
+__global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* __restrict__ part, double kappa,
                                                      int* __restrict__ band64, double* __restrict__ ratio) {
     __shared__ double sh[2][256];
     double s2 = 0.0, e2 = 0.0;
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* _
     }
     if (threadIdx.x == 0) {
         const double S2 = sh[0][0], E2 = sh[1][0];
-        *band64 = (!(E2 > 0.0) || kBandKappa * kBandKappa * S2 > kBandBudget * kBandBudget * E2) ? 1 : 0;
+        *band64 = (!(E2 > 0.0) || kappa * kappa * S2 > kBandBudget * kBandBudget * E2) ? 1 : 0;
         *ratio = E2 > 0.0 ? sqrt(S2 / E2) : -1.0;
     }
 }
@@ -516,6 +518,18 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                         const float2 r2 = __ffma2_rn(d, d, e2v);
                         const float qW = e.z * rcp_approx(r2.x * r2.y);
                         acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
+                    }
+                }
+                // In the accurate mode (small fields) the FP32 sums restart every
+                // 32 sources, their values moved into the FP64 accumulators: the
+                // rounding of a sequential FP32 sum grows like n^1.5, so 8 short
+                // sums instead of one of 256 terms round about 8x less.
+                if (b64 && (j0 & 31) == 24) {
+#pragma unroll
+                    for (int h = 0; h < kR / 2; ++h) {
+                        acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
+                        acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
+                        acc2[h] = make_float2(0.f, 0.f);
                     }
                 }
             }
@@ -839,7 +853,8 @@ class Direct32c final : public FieldEngine {
         // band arithmetic of this evaluation (a device flag: nothing waits on the host)
         if (band_mode_ == 2 && eref_ && eref_n_ == nt) {
             k_band_stats<<<kBandStatBlocks, 256, 0, st>>>(nt, info_.p, pq2_.p, ns, tperm, eref_, bandpart_.p);
-            k_band_decide<<<1, 256, 0, st>>>(kBandStatBlocks, bandpart_.p, band64_.p, bandratio_.p);
+            const double kappa = kBandKappa0 * (1.0 + kBandSpan * L_ / ((double)ntiles * eps_));
+            k_band_decide<<<1, 256, 0, st>>>(kBandStatBlocks, bandpart_.p, kappa, band64_.p, bandratio_.p);
             FS_LAUNCHED(2);
         } else {
             FS_CUDA(cudaMemsetAsync(band64_.p, band_mode_ == 0 ? 0 : 1, sizeof(int), st));  // any non-zero byte: FP64

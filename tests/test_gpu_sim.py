@@ -279,3 +279,21 @@ def test_boost_initial_conditions_in_session(ics, keys, dom):
     g.step(2)
     assert np.all(np.isfinite(g.state()["xs"]))
     g.close()
+
+
+def test_two_species_landau_config_reports_the_reference_shift_failure():
+    """At the step-20 remesh of the two-species Landau configuration the
+    reference throws "too many shifts!" (tests/test_oracle_reference_sim.py);
+    the device session returns FS_ERR_SHIFT at that step, after 19 steps that
+    match the restatement."""
+    d = decks.landau_two_species(h=5, ph=1, steps=20)
+    g = M.Simulation(d, "direct64")
+    g.step(19)
+    o = O.Sim(d)
+    o.step(19)
+    a, b = g.state(), o.state()
+    assert rel(a["fs"], b["fs"]) < 1e-11 and rel(a["xs"], b["xs"]) < 1e-11
+    with pytest.raises(M.FsError) as e:
+        g.step(1)
+    assert e.value.code == 5  # FS_ERR_SHIFT
+    g.close()

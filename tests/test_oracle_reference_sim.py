@@ -190,3 +190,26 @@ def test_initial_conditions_match_reference(name, sp, xr, pr):
         assert np.max(np.abs(ora - ref) / np.maximum(np.abs(ref), 1e-300)) <= 1e-13
     else:
         assert np.array_equal(ora, ref)
+
+
+def test_two_species_landau_config_remesh_fails_at_step_20_in_the_reference():
+    """The two-species Landau configuration (32 x 64 panels per species, dt 0.5,
+    remesh every 5 steps) cannot run its 20 steps in the reference: at the
+    step-20 remesh shift_xs needs more than ten periodic shifts for a point of
+    the cold ion species and throws ("too many shifts!",
+    AMRStructure_interp.cpp:429-491).  The restatement stops at the same step;
+    the device session reports FS_ERR_SHIFT there (tests/test_gpu_sim.py)."""
+    d = decks.landau_two_species(h=5, ph=1, steps=20)
+    r, o = O.RefSim(d), O.Sim(d)
+    try:
+        r.step(19)
+        o.step(19)
+        a, b = r.state(), o.state()
+        for key in KEYS:
+            assert np.array_equal(a[key], b[key]), key
+        with pytest.raises(RuntimeError):
+            r.step()
+        with pytest.raises(RuntimeError):
+            o.step()
+    finally:
+        r.close()
