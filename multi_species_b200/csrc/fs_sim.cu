@@ -81,15 +81,21 @@ __global__ void k_rk_stage1(int n, Stage S, double* __restrict__ e, double* __re
 // ---------------------------------------------------------------- 9-point fit
 // Row pivoting by the largest |a| (first on ties); the algorithm class of the
 // reference's Eigen PartialPivLU (AMRStructure_interp.cpp:935).
-__device__ void lu_solve9(double A[9][9], double b[9]) {
-    int perm[9];
+// The 9x9 solve of one leaf, in the thread's own slice of shared memory (the
+// partial pivoting swaps rows at run time; in registers that indexing would
+// put the matrix in local memory, which for a leaf per thread spills to DRAM).
+// A[i][j] = a[9 i + j]; b holds the right-hand side, then the solution.
+// Partial pivoting by the largest |a| (first index on ties), the algorithm of
+// Eigen's PartialPivLU (AMRStructure_interp.cpp:935), one rounding per
+// operation.
+__device__ void lu_solve9(double* a, double* b, int* perm) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) perm[i] = i;
     for (int k = 0; k < 9; ++k) {
         int piv = k;
-        double best = fabs(A[k][k]);
+        double best = fabs(a[9 * k + k]);
         for (int i = k + 1; i < 9; ++i) {
-            const double v = fabs(A[i][k]);
+            const double v = fabs(a[9 * i + k]);
             if (v > best) {
                 best = v;
                 piv = i;
@@ -97,57 +103,79 @@ __device__ void lu_solve9(double A[9][9], double b[9]) {
         }
         if (piv != k) {
             for (int j = 0; j < 9; ++j) {
-                const double t = A[k][j];
-                A[k][j] = A[piv][j];
-                A[piv][j] = t;
+                const double t = a[9 * k + j];
+                a[9 * k + j] = a[9 * piv + j];
+                a[9 * piv + j] = t;
             }
             const int t = perm[k];
             perm[k] = perm[piv];
             perm[piv] = t;
         }
         if (best != 0.0)
-            for (int i = k + 1; i < 9; ++i) A[i][k] = ddiv(A[i][k], A[k][k]);
+            for (int i = k + 1; i < 9; ++i) a[9 * i + k] = ddiv(a[9 * i + k], a[9 * k + k]);
         for (int i = k + 1; i < 9; ++i)
-            for (int j = k + 1; j < 9; ++j) A[i][j] = dsub(A[i][j], dmul(A[i][k], A[k][j]));
+            for (int j = k + 1; j < 9; ++j) a[9 * i + j] = dsub(a[9 * i + j], dmul(a[9 * i + k], a[9 * k + j]));
     }
     double y[9];
+#pragma unroll
     for (int i = 0; i < 9; ++i) y[i] = b[perm[i]];
+#pragma unroll
     for (int k = 0; k < 9; ++k)
-        for (int i = k + 1; i < 9; ++i) y[i] = dsub(y[i], dmul(y[k], A[i][k]));
+#pragma unroll
+        for (int i = k + 1; i < 9; ++i) y[i] = dsub(y[i], dmul(y[k], a[9 * i + k]));
+#pragma unroll
     for (int k = 8; k >= 0; --k) {
-        y[k] = ddiv(y[k], A[k][k]);
-        for (int i = 0; i < k; ++i) y[i] = dsub(y[i], dmul(y[k], A[i][k]));
+        y[k] = ddiv(y[k], a[9 * k + k]);
+#pragma unroll
+        for (int i = 0; i < k; ++i) y[i] = dsub(y[i], dmul(y[k], a[9 * i + k]));
     }
+#pragma unroll
     for (int i = 0; i < 9; ++i) b[i] = y[i];
 }
 
-// coef[slot*11 + 0..8] = c, [9] = x4, [10] = p4
-__global__ void k_panel_fit(int nleaves, const int* __restrict__ leaves, const int* __restrict__ rec,
-                            const double* __restrict__ ox, const double* __restrict__ op,
-                            const double* __restrict__ of, double* __restrict__ coef) {
+// Shared memory of one thread of k_panel_fit: the matrix, the right-hand side
+// and the row permutation.
+constexpr int kFitThreads = 64;
+constexpr size_t kFitSmemPerThread = (81 + 9) * sizeof(double) + 9 * sizeof(int);
+
+// Per leaf: the 9 old points' (x, p, f), the monomial basis
+// {1, dx, dx dp, dp, dx^2, dx^2 dp, dx^2 dp^2, dx dp^2, dp^2} about point 4,
+// and the 11-double fit record (9 coefficients, centre x, p)
+// (interpolate_from_panel_to_points, AMRStructure_interp.cpp:795-975).
+__global__ void __launch_bounds__(kFitThreads) k_panel_fit(int nleaves, const int* __restrict__ leaves,
+                                                           const int* __restrict__ rec, const double* __restrict__ ox,
+                                                           const double* __restrict__ op,
+                                                           const double* __restrict__ of, double* __restrict__ coef) {
+    extern __shared__ __align__(16) unsigned char fit_smem[];
+    double* a = reinterpret_cast<double*>(fit_smem) + (size_t)threadIdx.x * 81;
+    double* c = reinterpret_cast<double*>(fit_smem) + (size_t)kFitThreads * 81 + (size_t)threadIdx.x * 9;
+    int* perm = reinterpret_cast<int*>(fit_smem + (size_t)kFitThreads * 90 * sizeof(double)) + threadIdx.x * 9;
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nleaves) return;
     const int* r = rec + (size_t)leaves[l] * 18;
-    double px[9], pp[9], A[9][9], c[9];
+    double px[9], pp[9];
+#pragma unroll
     for (int i = 0; i < 9; ++i) {
         px[i] = ox[r[i]];
         pp[i] = op[r[i]];
         c[i] = of[r[i]];
     }
+#pragma unroll
     for (int i = 0; i < 9; ++i) {
         const double dx = dsub(px[i], px[4]), dp = dsub(pp[i], pp[4]);
-        A[i][0] = 1;
-        A[i][1] = dx;
-        A[i][2] = dmul(dx, dp);
-        A[i][3] = dp;
-        A[i][4] = dmul(dx, dx);
-        A[i][5] = dmul(dmul(dx, dx), dp);
-        A[i][6] = dmul(dmul(dmul(dx, dx), dp), dp);
-        A[i][7] = dmul(dmul(dx, dp), dp);
-        A[i][8] = dmul(dp, dp);
+        a[9 * i + 0] = 1;
+        a[9 * i + 1] = dx;
+        a[9 * i + 2] = dmul(dx, dp);
+        a[9 * i + 3] = dp;
+        a[9 * i + 4] = dmul(dx, dx);
+        a[9 * i + 5] = dmul(dmul(dx, dx), dp);
+        a[9 * i + 6] = dmul(dmul(dmul(dx, dx), dp), dp);
+        a[9 * i + 7] = dmul(dmul(dx, dp), dp);
+        a[9 * i + 8] = dmul(dp, dp);
     }
-    lu_solve9(A, c);
+    lu_solve9(a, c, perm);
     double* o = coef + (size_t)l * 11;
+#pragma unroll
     for (int i = 0; i < 9; ++i) o[i] = c[i];
     o[9] = px[4];
     o[10] = pp[4];
@@ -477,8 +505,13 @@ __global__ void k_leaf_xmid(int ncell, const int* __restrict__ leaf_grid, const 
 }
 
 // Guess of the old leaf holding each sorted slot: its p-row by p, then the
-// leaf of that row whose centre is nearest in x, periodically.
-__global__ void k_guess(int n, const double* __restrict__ sortx, const double* __restrict__ sortp, double pmin,
+// leaf of that row whose centre is nearest in x, periodically; then a short
+// walk from there (at most kGuessWalk panels) onto the panel the edge tests
+// select -- lattice points on a row boundary belong to the row above or
+// below depending on how the old boundary moved.
+constexpr int kGuessWalk = 8;
+__global__ void k_guess(MeshView M, const double* __restrict__ ox, const double* __restrict__ op, int n,
+                        const double* __restrict__ sortx, const double* __restrict__ sortp, double pmin,
                         double dpp, int npx, int npp, double Lx, const double* __restrict__ xmid,
                         const int* __restrict__ leaf_grid, int* __restrict__ guess) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -499,7 +532,12 @@ __global__ void k_guess(int n, const double* __restrict__ sortx, const double* _
     if (ix < 0) ix = 0;
     const double right = (ix + 1 < npx) ? (xm[ix + 1] - x0) : Lx;
     if (right - u < u - (xm[ix] - x0)) ix = (ix + 1) % npx;
-    guess[k] = leaf_grid[(size_t)ip * npx + ix];
+    const int g = leaf_grid[(size_t)ip * npx + ix];
+    int hist[kGuessWalk];
+    bool beyond = false;
+    double tx = sortx[k];
+    const int w = walk_from(M, ox, op, tx, sortp[k], g, beyond, hist, min(kGuessWalk, g_walk_limit));
+    guess[k] = w >= 0 ? w : g;
 }
 
 // Every sorted slot's walk from the guess for its predecessor (slot 0: from
@@ -1367,8 +1405,8 @@ struct Sim {
             const int a = s->start;
             const int nb = s->nbase;
             ProfScope prof("remesh", st);
-            k_panel_fit<<<blocks(s->nleaves, 128), 128, 0, st>>>(s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a,
-                                                            f.p + a, s->coef.p);
+            k_panel_fit<<<blocks(s->nleaves, kFitThreads), kFitThreads, kFitThreads * kFitSmemPerThread, st>>>(
+                s->nleaves, s->leaves.p, s->rec.p, x.p + a, p.p + a, f.p + a, s->coef.p);
             const MeshView M = mesh_view(*s);
             k_shift<<<blocks(nb), kT, 0, st>>>(nb, s->lat_x.p, s->lat_p.p, L, x.p + a, p.p + a, s->sx.p, status.p);
             const size_t smem = (size_t)s->pow2 * (sizeof(double) + sizeof(int));
@@ -1379,8 +1417,8 @@ struct Sim {
             if (s->grid_ok) {
                 const int ncell = s->npx * s->npp;
                 k_leaf_xmid<<<blocks(ncell), kT, 0, st>>>(ncell, s->leaf_grid.p, s->rec.p, x.p + a, s->xmid.p);
-                k_guess<<<blocks(nb), kT, 0, st>>>(nb, s->sortx.p, s->sortp.p, M.pmin, M.dpp, s->npx, s->npp, L,
-                                                   s->xmid.p, s->leaf_grid.p, s->wG.p);
+                k_guess<<<blocks(nb, 128), 128, 0, st>>>(M, x.p + a, p.p + a, nb, s->sortx.p, s->sortp.p, M.pmin,
+                                                         M.dpp, s->npx, s->npp, L, s->xmid.p, s->leaf_grid.p, s->wG.p);
                 k_walk_spec<<<blocks(nb, 128), 128, 0, st>>>(M, s->nxl, nb, x.p + a, p.p + a, s->sortx.p, s->sortp.p,
                                                              s->wG.p, s->wR.p, s->wS.p, s->wB.p, s->wTX.p, s->wroot.p,
                                                              s->wroot_x.p, status.p);
