@@ -231,6 +231,14 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // are used when kappa ||S|| stays below kBandBudget times the previous
 // field's norm (the field changes little between evaluations), FP64 band
 // terms otherwise or when no previous field is known.
+#ifndef FS_FAR_FLUSH
+#define FS_FAR_FLUSH 1
+#endif
+constexpr bool kFarFlush = FS_FAR_FLUSH;
+#ifndef FS_BAND64
+#define FS_BAND64 1
+#endif
+constexpr bool kBand64 = FS_BAND64;  // 0: the FP64 band branch is compiled out (measurements only)
 constexpr double kBandKappa0 = 6e-8;
 constexpr double kBandSpan = 0.15;
 constexpr double kBandBudget = 4e-7;
@@ -347,7 +355,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
     constexpr uint32_t kBytes = kS * sizeof(float4);
     constexpr uint32_t kBytes64 = kS * sizeof(double2);
     const long long polls = g_mbar_polls;
-    const bool b64 = *Jb.band64 != 0;  // the job's band arithmetic, decided on the device
+    const bool b64 = kBand64 && *Jb.band64 != 0;  // the job's band arithmetic, decided on the device
     if (tid == 0) {
         fence_proxy_async();
         mbar_expect_tx(&bar[gk & 1], kBytes + kBytes64);
@@ -524,7 +532,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 // 32 sources, their values moved into the FP64 accumulators: the
                 // rounding of a sequential FP32 sum grows like n^1.5, so 8 short
                 // sums instead of one of 256 terms round about 8x less.
-                if (b64 && (j0 & 31) == 24) {
+                if (kFarFlush && b64 && (j0 & 31) == 24) {
 #pragma unroll
                     for (int h = 0; h < kR / 2; ++h) {
                         acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
