@@ -33,10 +33,6 @@ struct fs_field {
     std::unique_ptr<fsb::FieldEngine> engine;
     cudaStream_t st = nullptr;
     fsb::DevBuf<double> t, s, q, e;
-    // e holds the previous call's E at `last_nt` targets (the same points,
-    // moved, in a simulation's successive calls) while e.p == last_e
-    int last_nt = -1;
-    const double* last_e = nullptr;
     ~fs_field() {
         if (st) cudaStreamDestroy(st);
     }
@@ -120,16 +116,11 @@ fs_status fs_field_eval(fs_field* field, double* es, const double* targets, int 
         fsb::Stage S;
         S.kind = fsb::STAGE_STORE;
         S.out = field->e.p;
-        const bool prev = field->last_nt == nt && field->last_e == field->e.p;
-        field->engine->set_reference_field(prev ? field->e.p : nullptr, nt);
-        field->last_nt = -1;
         if (nt) {
             field->engine->eval(same ? field->s.p : field->t.p, nt, field->s.p, field->q.p, ns, S, st);
             FS_CUDA(cudaMemcpyAsync(es, field->e.p, sizeof(double) * nt, cudaMemcpyDeviceToHost, st));
         }
         field->check_errors(st);
-        field->last_nt = nt;
-        field->last_e = field->e.p;
     });
 }
 
@@ -141,8 +132,6 @@ fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_ta
         if (tree && nt != ns) fsb::fail(FS_ERR_ARG, "treecode evaluates at the sources: nt must equal ns");
         FS_CUDA(cudaSetDevice(field->prm.device));
         cudaStream_t st = stream ? (cudaStream_t)stream : field->st;
-        field->engine->set_reference_field(nullptr, 0);  // caller memory: no previous field known
-        field->last_nt = -1;
         fsb::Stage S;
         S.kind = fsb::STAGE_STORE;
         S.out = d_es;

@@ -137,7 +137,7 @@ __global__ void k_wrap_keys(const double* __restrict__ x, int n, double L, uint6
 __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* __restrict__ sidx,
                                  const double* __restrict__ q, int ns, int ns_pad, double a1, double a2,
                                  float4* __restrict__ src, double2* __restrict__ src64, double* __restrict__ tbase,
-                                 double* __restrict__ qs, double* __restrict__ qx, double* __restrict__ q2) {
+                                 double* __restrict__ qs, double* __restrict__ qx) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns_pad) return;
     if (j >= ns) {
@@ -153,7 +153,6 @@ __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* 
     src[j] = make_float4((float)(xj - base), qh, (float)((double)qh * a1), (float)((double)qh * a2));
     src64[j] = make_double2(xj, 0.5 * qj);
     qs[j] = qj;
-    q2[j] = 0.25 * qj * qj;  // (q/2)^2, summed over each target's band by the band-mode estimate
     qx[j] = qj * xj;
 }
 
@@ -221,84 +220,21 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
     info[i] = T;
 }
 
-// Band arithmetic per evaluation.  Summed in FP32, band terms (O(q/2) each)
-// leave an error in E of about kappa * ||S||, S_i^2 = the sum of (q_j/2)^2 over
-// target i's band -- the terms cancel to the field, their roundings do not.
-// kappa grows with the tile span in units of eps (the FP32 tile-relative
-// coordinates round in proportion to the span): measured on B200 against the
-// FP64 sum over two-stream, two-species Landau and 2k-66k-point batch decks,
-// kappa <= 6e-8 (1 + 0.15 L / (ntiles eps)) in every case.  FP32 band terms
-// are used when kappa ||S|| stays below kBandBudget times the previous
-// field's norm (the field changes little between evaluations), FP64 band
-// terms otherwise or when no previous field is known.
-#ifndef FS_FAR_FLUSH
-#define FS_FAR_FLUSH 1
+// Far tiles restart their FP32 sums every kFarChunk sources (0: one sum per
+// tile), moving the partial sums into the FP64 accumulators: the rounding of a
+// sequential FP32 sum of n similar terms grows like n^1.5.
+#ifndef FS_FAR_CHUNK
+#define FS_FAR_CHUNK 32
 #endif
-constexpr bool kFarFlush = FS_FAR_FLUSH;
-#ifndef FS_BAND64
-#define FS_BAND64 1
+constexpr int kFarChunk = FS_FAR_CHUNK;
+static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "far chunk: a multiple of 8 dividing 256");
+// FP64 source records for the band pairs: staged into shared memory with the
+// FP32 ones (1), or read from global memory by the band and mixed tiles that
+// need them (0).
+#ifndef FS_STAGE64
+#define FS_STAGE64 1
 #endif
-constexpr bool kBand64 = FS_BAND64;  // 0: the FP64 band branch is compiled out (measurements only)
-constexpr double kBandKappa0 = 6e-8;
-constexpr double kBandSpan = 0.15;
-constexpr double kBandBudget = 4e-7;
-constexpr int kBandStatBlocks = 296;
-
-// Per block: partial sums over targets of S_i^2 and of the previous E_i^2.
-__global__ void __launch_bounds__(256) k_band_stats(int nt, const TargetInfo* __restrict__ info,
-                                                    const double* __restrict__ pq2, int ns,
-                                                    const int* __restrict__ tperm, const double* __restrict__ eref,
-                                                    double* __restrict__ part) {
-    __shared__ double sh[2][256];
-    double s2 = 0.0, e2 = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x) {
-        const TargetInfo T = info[i];
-        s2 += unrolled_prefix(pq2, ns, T.U2) - unrolled_prefix(pq2, ns, T.U1);
-        const double ev = eref[tperm[i]];
-        e2 += ev * ev;
-    }
-    sh[0][threadIdx.x] = s2;
-    sh[1][threadIdx.x] = e2;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = sh[0][0];
-        part[2 * blockIdx.x + 1] = sh[1][0];
-    }
-}
-
-// One block: the sums in a fixed order, the decision, and sqrt(S2 / E2) for
-// diagnostics.
-__global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* __restrict__ part, double kappa,
-                                                     int* __restrict__ band64, double* __restrict__ ratio) {
-    __shared__ double sh[2][256];
-    double s2 = 0.0, e2 = 0.0;
-    for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
-        s2 += part[2 * b];
-        e2 += part[2 * b + 1];
-    }
-    sh[0][threadIdx.x] = s2;
-    sh[1][threadIdx.x] = e2;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const double S2 = sh[0][0], E2 = sh[1][0];
-        *band64 = (!(E2 > 0.0) || kappa * kappa * S2 > kBandBudget * kBandBudget * E2) ? 1 : 0;
-        *ratio = E2 > 0.0 ? sqrt(S2 / E2) : -1.0;
-    }
-}
+constexpr bool kStage64 = FS_STAGE64;
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
 // v = eps^2 w, w = 1/(d^2 + eps^2), v <= 1/(1 + kBand^2).  The sign part is
@@ -313,12 +249,6 @@ __global__ void __launch_bounds__(256) k_band_decide(int nparts, const double* _
 #define FS_PAIR_BAND 16.0
 #endif
 constexpr double kBand = FS_PAIR_BAND;  // near band half-width in units of eps
-// Far tiles: bit k set = the k-th source of each eight-source body uses one
-// reciprocal per four targets instead of one per two (see the far loop).
-#ifndef FS_QUAD_MASK
-#define FS_QUAD_MASK 0x00
-#endif
-constexpr unsigned kQuadMask = FS_QUAD_MASK;
 constexpr int kMaxChunks = 64;
 
 // One (target block, source chunk) of a job: kR targets per thread, the
@@ -353,14 +283,13 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
     // each tile: the FP32 records and the FP64 records of the same sources,
     // two bulk copies completing on one barrier
     constexpr uint32_t kBytes = kS * sizeof(float4);
-    constexpr uint32_t kBytes64 = kS * sizeof(double2);
+    constexpr uint32_t kBytes64 = kStage64 ? kS * sizeof(double2) : 0;
     const long long polls = g_mbar_polls;
-    const bool b64 = kBand64 && *Jb.band64 != 0;  // the job's band arithmetic, decided on the device
     if (tid == 0) {
         fence_proxy_async();
         mbar_expect_tx(&bar[gk & 1], kBytes + kBytes64);
         bulk_load(buf[gk & 1], Jb.src + (size_t)t0 * kS, kBytes, &bar[gk & 1]);
-        bulk_load(buf64[gk & 1], Jb.src64 + (size_t)t0 * kS, kBytes64, &bar[gk & 1]);
+        if (kStage64) bulk_load(buf64[gk & 1], Jb.src64 + (size_t)t0 * kS, kBytes64, &bar[gk & 1]);
     }
     for (int t = t0; t < t1; ++t, ++gk) {
         const int b = gk & 1;
@@ -368,7 +297,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             fence_proxy_async();
             mbar_expect_tx(&bar[b ^ 1], kBytes + kBytes64);
             bulk_load(buf[b ^ 1], Jb.src + (size_t)(t + 1) * kS, kBytes, &bar[b ^ 1]);
-            bulk_load(buf64[b ^ 1], Jb.src64 + (size_t)(t + 1) * kS, kBytes64, &bar[b ^ 1]);
+            if (kStage64) bulk_load(buf64[b ^ 1], Jb.src64 + (size_t)(t + 1) * kS, kBytes64, &bar[b ^ 1]);
         }
         const bool ok = mbar_wait_bounded(&bar[b], (gk >> 1) & 1, polls);
         if (!__syncthreads_and(ok)) {
@@ -411,12 +340,12 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             inband &= band;
         }
         const float4* tile = buf[b];
-        if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband) && b64) {
+        if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband)) {
             // band tiles (every pair of the warp within |d| <= band, one image
-            // per target), FP64 mode: q/2 * d / sqrt(d^2 + eps^2) from the FP64
+            // per target): q/2 * d / sqrt(d^2 + eps^2) in FP64 from the FP64
             // records.  Band terms are O(q/2) and cancel to the (possibly much
             // smaller) field; FP64 keeps their rounding below the field's size.
-            const double2* tile64 = buf64[b];
+            const double2* tile64 = kStage64 ? buf64[b] : Jb.src64 + (size_t)jlo;
             const double e2d = Jb.eps2d;
             double T[kR];
 #pragma unroll
@@ -430,44 +359,6 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                     acc64[r] = fma(e.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
                 }
             }
-        } else if (__any_sync(0xffffffffu, careful) && __all_sync(0xffffffffu, inband)) {
-            // band tiles, FP32 mode (the field is large enough for FP32 band
-            // terms): q/2 * d * y with y = rsqrt(d^2 + eps^2), two targets per
-            // packed FP32x2 op, Kahan-compensated
-            const float2 e2b = make_float2(eps2, eps2), m1 = make_float2(-1.f, -1.f);
-            float2 tau2[kR / 2], acc2[kR / 2], ncmp2[kR / 2];
-#pragma unroll
-            for (int h = 0; h < kR / 2; ++h) {
-                tau2[h] = make_float2(tau[2 * h], tau[2 * h + 1]);
-                acc2[h] = make_float2(0.f, 0.f);
-                ncmp2[h] = make_float2(0.f, 0.f);
-            }
-#pragma unroll 4
-            for (int j = 0; j < kS; ++j) {
-                const float4 e = tile[j];
-                const float2 sx2 = make_float2(e.x, e.x);
-                const float2 qh = make_float2(e.y, e.y);
-#pragma unroll
-                for (int h = 0; h < kR / 2; ++h) {
-                    // differences as FMAs with -1 (exact products), so no sign
-                    // flips are needed: d = tau - s, then Kahan with the
-                    // negated compensation nc = -c
-                    const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
-                    const float2 r2 = __ffma2_rn(d, d, e2b);
-                    const float2 y = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                    const float2 g = __fmul2_rn(d, y);
-                    const float2 v = __ffma2_rn(qh, g, ncmp2[h]);
-                    const float2 sum = __fadd2_rn(acc2[h], v);
-                    const float2 t = __ffma2_rn(acc2[h], m1, sum);
-                    ncmp2[h] = __ffma2_rn(t, m1, v);
-                    acc2[h] = sum;
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < kR / 2; ++h) {
-                acc64[2 * h] += (double)acc2[h].x + (double)ncmp2[h].x;
-                acc64[2 * h + 1] += (double)acc2[h].y + (double)ncmp2[h].y;
-            }
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
             // two targets per packed FP32x2 op, one MUFU.RCP per two targets
@@ -479,78 +370,45 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 acc2[h] = make_float2(0.f, 0.f);
             }
             // Eight sources per unrolled body (unroll 4 measured 3.5% slower,
-            // 16 no faster).  Each group of four targets uses, per source
-            // position k of the body, either two pair reciprocals (bit k of
-            // kQuadMask clear) or one quad reciprocal (bit set):
-            //   pair: 8 FP32 lane-ops and 1 MUFU.RCP per 2 pairs (4 lane-ops
-            //         and 0.5 MUFU per pair), which load the FMA
-            //         pipe and MUFU equally;
-            //   quad: 18 lane-ops and 1 MUFU.RCP per 4 pairs (4.5 and 0.25 per
-            //         pair), which moves work from MUFU to the FMA pipe.
-            // Mixing the two lets one pipe bound the loop with slack on the other.
+            // 16 no faster); per two targets one reciprocal and one scalar
+            // product: q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b), i.e.
+            // 4 FP32 lane-ops and 0.5 MUFU.RCP per pair, which load the FMA pipe
+            // and MUFU equally.  (One reciprocal per four targets -- 4.5
+            // lane-ops and 0.25 MUFU per pair -- mixed in for 1/8 to 1/2 of the
+            // sources measured 0.5-3.7% slower.)  The FP32 sums are moved into
+            // the FP64 accumulators every kFarChunk sources.
+            constexpr int kChunk = kFarChunk ? kFarChunk : kS;
 #pragma unroll 1
-            for (int j0 = 0; j0 < kS; j0 += 8) {
+            for (int c = 0; c < kS; c += kChunk) {
+#pragma unroll 1
+                for (int j0 = c; j0 < c + kChunk; j0 += 8) {
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const float4 e = tile[j0 + k];
-                    const float2 sx2 = make_float2(e.x, e.x);
+                    for (int k = 0; k < 8; ++k) {
+                        const float4 e = tile[j0 + k];
+                        const float2 sx2 = make_float2(e.x, e.x);
 #pragma unroll
-                    for (int g = 0; g < kR / 4; ++g) {
-                        const int h0 = 2 * g, h1 = 2 * g + 1;
-                        const float2 d0 = __ffma2_rn(sx2, m1, tau2[h0]);  // tau - s, exact product by -1
-                        const float2 d1 = __ffma2_rn(sx2, m1, tau2[h1]);
-                        const float2 r0 = __ffma2_rn(d0, d0, e2v);
-                        const float2 r1 = __ffma2_rn(d1, d1, e2v);
-                        if ((kQuadMask >> k) & 1) {
-                            // q/2 a1 / r_a = (q/2 a1 W) r_b r_c r_d with
-                            // W = 1/(r_a r_b r_c r_d): one reciprocal for four targets
-                            const float pab = r0.x * r0.y, pcd = r1.x * r1.y;
-                            const float qW = e.z * rcp_approx(pab * pcd);
-                            const float wab = qW * pcd, wcd = qW * pab;
-                            acc2[h0] = __ffma2_rn(r0, make_float2(wab, wab), acc2[h0]);
-                            acc2[h1] = __ffma2_rn(r1, make_float2(wcd, wcd), acc2[h1]);
-                        } else {
-                            // q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b): one
-                            // reciprocal and one scalar product serve both targets
-                            const float qW0 = e.z * rcp_approx(r0.x * r0.y);
-                            const float qW1 = e.z * rcp_approx(r1.x * r1.y);
-                            acc2[h0] = __ffma2_rn(r0, make_float2(qW0, qW0), acc2[h0]);
-                            acc2[h1] = __ffma2_rn(r1, make_float2(qW1, qW1), acc2[h1]);
+                        for (int h = 0; h < kR / 2; ++h) {
+                            const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
+                            const float2 r2 = __ffma2_rn(d, d, e2v);
+                            const float qW = e.z * rcp_approx(r2.x * r2.y);
+                            acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
                         }
-                        // (w r_a, w r_b) are the terms of targets 2h+1 and 2h:
-                        // acc2[h].x accumulates target 2h+1 and .y target 2h
-                    }
-#pragma unroll
-                    for (int h = 2 * (kR / 4); h < kR / 2; ++h) {  // a last pair of targets (kR = 2)
-                        const float2 d = __ffma2_rn(sx2, m1, tau2[h]);
-                        const float2 r2 = __ffma2_rn(d, d, e2v);
-                        const float qW = e.z * rcp_approx(r2.x * r2.y);
-                        acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
                     }
                 }
-                // In the accurate mode (small fields) the FP32 sums restart every
-                // 32 sources, their values moved into the FP64 accumulators: the
-                // rounding of a sequential FP32 sum grows like n^1.5, so 8 short
-                // sums instead of one of 256 terms round about 8x less.
-                if (kFarFlush && b64 && (j0 & 31) == 24) {
+                // (qW r_a, qW r_b) are the terms of targets 2h+1 and 2h:
+                // acc2[h].x holds target 2h+1 and .y target 2h
 #pragma unroll
-                    for (int h = 0; h < kR / 2; ++h) {
-                        acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
-                        acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
-                        acc2[h] = make_float2(0.f, 0.f);
-                    }
+                for (int h = 0; h < kR / 2; ++h) {
+                    acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
+                    acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
+                    acc2[h] = make_float2(0.f, 0.f);
                 }
-            }
-#pragma unroll
-            for (int h = 0; h < kR / 2; ++h) {
-                acc64[2 * h] -= (double)sg[2 * h] * (double)acc2[h].y;
-                acc64[2 * h + 1] -= (double)sg[2 * h + 1] * (double)acc2[h].x;
             }
         } else {
             // near band / image split: per-pair image and band; band pairs
-            // q/2 * d / sqrt(d^2 + eps^2) in FP64 or FP32 (as in band tiles),
-            // far pairs -+ q/2 * c in FP32, FP32 terms with a Kahan sum
-            const double2* tile64 = buf64[b];
+            // q/2 * d / sqrt(d^2 + eps^2) in FP64 (as in band tiles), far pairs
+            // -+ q/2 * c in FP32 with a Kahan sum
+            const double2* tile64 = kStage64 ? buf64[b] : Jb.src64 + (size_t)jlo;
             const double e2d = Jb.eps2d;
             float cmp[kR];
 #pragma unroll
@@ -562,17 +420,10 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                 for (int r = 0; r < kR; ++r) {
                     const bool lo_img = idx < J[r];
                     const int u = lo_img ? idx + ns : idx;
-                    if (u >= U1[r] && u < U2[r] && b64) {
+                    if (u >= U1[r] && u < U2[r]) {
                         const double2 e64 = tile64[j];
                         const double d = (lo_img ? tl[r] : tl[r] + L) - e64.x;
                         acc64[r] = fma(e64.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
-                    } else if (u >= U1[r] && u < U2[r]) {
-                        const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
-                        const float y = rsqrt_approx(fmaf(d, d, eps2));
-                        const float v = fmaf(e.y, d * y, -cmp[r]);
-                        const float sum = acc[r] + v;
-                        cmp[r] = (sum - acc[r]) - v;
-                        acc[r] = sum;
                     } else {
                         const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
                         const float y = rsqrt_approx(fmaf(d, d, eps2));
@@ -762,28 +613,8 @@ class Direct32c final : public FieldEngine {
             const int r = std::atoi(v);
             if (r == 2 || r == 4 || r == 8) R_ = r;
         }
-        // band arithmetic: automatic (default), or forced FP32 ("0") / FP64 ("1")
-        // for measurements of the two
-        if (const char* v = std::getenv("FS_B200_BAND64")) {
-            if (v[0] == '0') band_mode_ = 0;
-            if (v[0] == '1') band_mode_ = 1;
-        }
     }
 
-    void set_reference_field(const double* e, int n) override {
-        eref_ = e;
-        eref_n_ = n;
-    }
-
-    // sqrt(S2 / E2) of the last automatic band decision (-1: none), for diagnostics
-    double last_band_ratio(cudaStream_t st) {
-        double r = -1.0;
-        if (bandratio_.p) {
-            FS_CUDA(cudaMemcpyAsync(&r, bandratio_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
-            FS_CUDA(cudaStreamSynchronize(st));
-        }
-        return r;
-    }
 
     void eval(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
               cudaStream_t st) override {
@@ -828,11 +659,9 @@ class Direct32c final : public FieldEngine {
             FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_.p, tb, kin_.p, kout_.p, iin_.p, iout_.p, ns, 0, 63, st));
             k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
                                                                  e2 * e2 / 8, src_.p, src64_.p, tbase_.p, qs_.p,
-                                                                 qx_.p, q2_.p);
+                                                                 qx_.p);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
-            tb = cub_.bytes();
-            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, q2_.p, pq2_.p, ns, st));
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
             FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
@@ -858,17 +687,8 @@ class Direct32c final : public FieldEngine {
         k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_, pq_.p,
                                                          info_.p);
         FS_LAUNCHED(1);
-        // band arithmetic of this evaluation (a device flag: nothing waits on the host)
-        if (band_mode_ == 2 && eref_ && eref_n_ == nt) {
-            k_band_stats<<<kBandStatBlocks, 256, 0, st>>>(nt, info_.p, pq2_.p, ns, tperm, eref_, bandpart_.p);
-            const double kappa = kBandKappa0 * (1.0 + kBandSpan * L_ / ((double)ntiles * eps_));
-            k_band_decide<<<1, 256, 0, st>>>(kBandStatBlocks, bandpart_.p, kappa, band64_.p, bandratio_.p);
-            FS_LAUNCHED(2);
-        } else {
-            FS_CUDA(cudaMemsetAsync(band64_.p, band_mode_ == 0 ? 0 : 1, sizeof(int), st));  // any non-zero byte: FP64
-        }
         *job = PairJob{src_.p, src64_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
-                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, band64_.p};
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
         return true;
     }
 
@@ -891,8 +711,6 @@ class Direct32c final : public FieldEngine {
         iout_.ensure(ns);
         src_.ensure(ns_pad);
         src64_.ensure(ns_pad);
-        q2_.ensure(ns);
-        pq2_.ensure(ns);
         qs_.ensure(ns);
         qx_.ensure(ns);
         pq_.ensure(ns);
@@ -904,10 +722,6 @@ class Direct32c final : public FieldEngine {
             err_.ensure(1);
             FS_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
             counter_.ensure(1);
-            band64_.ensure(1);
-            bandratio_.ensure(1);
-            bandpart_.ensure(2 * kBandStatBlocks);
-            FS_CUDA(cudaMemset(bandratio_.p, 0, sizeof(double)));
         }
         const int nsort = std::max(ns, nt_sep);
         if (nt_sep) {
@@ -941,11 +755,6 @@ class Direct32c final : public FieldEngine {
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
     DevBuf<double2> src64_;
-    DevBuf<double> q2_, pq2_, bandpart_, bandratio_;
-    DevBuf<int> band64_;
-    int band_mode_ = 2;  // 0 FP32 band, 1 FP64 band, 2 automatic
-    const double* eref_ = nullptr;
-    int eref_n_ = 0;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
@@ -989,7 +798,7 @@ namespace {
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct NoAllocLayout {
-    size_t kin, kout, iin, iout, src, src64, q2, band64, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
+    size_t kin, kout, iin, iout, src, src64, tbase, qs, qx, pq, qxsum, info, partial, err, cub, total;
 };
 
 constexpr NoAllocLayout noalloc_layout() {
@@ -1002,8 +811,6 @@ constexpr NoAllocLayout noalloc_layout() {
     L.iout = o;    o += align256(n * sizeof(int));
     L.src = o;     o += align256(n * sizeof(float4));
     L.src64 = o;   o += align256(n * sizeof(double2));
-    L.q2 = o;      o += align256(n * sizeof(double));
-    L.band64 = o;  o += align256(sizeof(int));
     L.tbase = o;   o += align256((n / kS) * sizeof(double));
     L.qs = o;      o += align256(n * sizeof(double));
     L.qx = o;      o += align256(n * sizeof(double));
@@ -1068,8 +875,6 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     int* iout = reinterpret_cast<int*>(at(kNoAlloc.iout));
     float4* src = reinterpret_cast<float4*>(at(kNoAlloc.src));
     double2* src64 = reinterpret_cast<double2*>(at(kNoAlloc.src64));
-    double* q2 = reinterpret_cast<double*>(at(kNoAlloc.q2));
-    int* band64 = reinterpret_cast<int*>(at(kNoAlloc.band64));
     double* tbase = reinterpret_cast<double*>(at(kNoAlloc.tbase));
     double* qs = reinterpret_cast<double*>(at(kNoAlloc.qs));
     double* qx = reinterpret_cast<double*>(at(kNoAlloc.qx));
@@ -1105,15 +910,14 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     FS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, tb, kin, kout, iin, iout, n, 0, 63, st));
     const double e2 = eps * eps;
     k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, src64,
-                                                         tbase, qs, qx, q2);
-    FS_CUDA(cudaMemsetAsync(band64, 1, sizeof(int), st));  // no previous field here: band pairs in FP64
+                                                         tbase, qs, qx);
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
     const PairJob job{src, src64, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
-                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, band64};
+                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
     launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;

@@ -202,7 +202,6 @@ struct PairJob {
     float eps2, a1, a2;  // near band: eps^2, eps^2/2, eps^4/8
     float e2f;           // far pairs: 3 eps^2 / 4
     double eps2d;        // band pairs (FP64): eps^2
-    const int* band64;   // device flag: non-zero = band pairs in FP64, else FP32 with Kahan
 };
 
 class FieldEngine {
@@ -215,10 +214,6 @@ class FieldEngine {
                       int ns, const Stage& stage, cudaStream_t st) = 0;
     // Device int set non-zero by a kernel whose bounded wait gave up (or null).
     virtual int* error_flag() { return nullptr; }
-    // The field of the previous evaluation at the same n targets, by target
-    // index (device pointer, or null): engines that choose their arithmetic
-    // from the size of the field they compute read it.
-    virtual void set_reference_field(const double* e, int n) { (void)e; (void)n; }
     // Kernel-level evaluations of the last call (pairs for the direct sums;
     // near pairs + far cluster terms for the treecode).  May synchronise `st`;
     // called only when profiling is enabled.

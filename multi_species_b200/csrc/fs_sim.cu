@@ -1301,9 +1301,6 @@ struct Sim {
                 break;
             default: fail(FS_ERR_ARG, "unknown field kind");
         }
-        // the field chooses its band arithmetic from E of the previous
-        // evaluation at the same points (the end-of-step or reduced-grid field)
-        field->set_reference_field(e.p, N);
         base.x = x.p;
         base.p = p.p;
         base.pst = pst.p;
@@ -1528,7 +1525,6 @@ struct Sim {
         upload(f, af);
         upload(qw, aq);
         for (auto* b : {&e, &xkA, &xkB, &pst, &accX, &accP}) b->ensure(N);
-        if (field) field->set_reference_field(e.p, N);  // E of the previous evaluation, by point
         base.x = x.p;
         base.p = p.p;
         base.pst = pst.p;
