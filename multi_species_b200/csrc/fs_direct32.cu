@@ -108,9 +108,18 @@ __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_do
 
 // 1/sqrt(r) in FP64 for r > 0: the hardware approximation refined by one
 // Newton-Raphson step y (3/2 - r y^2 / 2), which squares its relative error.
+#ifndef FS_RSQ_SEED32
+#define FS_RSQ_SEED32 1
+#endif
 __device__ __forceinline__ double rsqrt_nr64(double r) {
     double y;
-    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
+    if (FS_RSQ_SEED32) {
+        // seed from the FP32 approximation (relative error below 2^-22 for the
+        // band's r in [eps^2, 257 eps^2], well inside FP32's range)
+        y = (double)rsqrt_approx((float)r);
+    } else {
+        asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
+    }
     const double t = y * y;
     const double u = fma(-0.5 * r, t, 1.5);
     return y * u;
@@ -224,7 +233,7 @@ __global__ void k_target_info(const uint64_t* __restrict__ tkeys, int nt, int nt
 // tile), moving the partial sums into the FP64 accumulators: the rounding of a
 // sequential FP32 sum of n similar terms grows like n^1.5.
 #ifndef FS_FAR_CHUNK
-#define FS_FAR_CHUNK 32
+#define FS_FAR_CHUNK 0
 #endif
 constexpr int kFarChunk = FS_FAR_CHUNK;
 static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "far chunk: a multiple of 8 dividing 256");
