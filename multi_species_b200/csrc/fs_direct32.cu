@@ -109,7 +109,7 @@ __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_do
 // 1/sqrt(r) in FP64 for r > 0: the hardware approximation refined by one
 // Newton-Raphson step y (3/2 - r y^2 / 2), which squares its relative error.
 #ifndef FS_RSQ_SEED32
-#define FS_RSQ_SEED32 1
+#define FS_RSQ_SEED32 0
 #endif
 __device__ __forceinline__ double rsqrt_nr64(double r) {
     double y;
@@ -243,6 +243,14 @@ static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "f
 #ifndef FS_STAGE64
 #define FS_STAGE64 1
 #endif
+// band tiles: sources per unrolled body, and two accumulators per target (1)
+#ifndef FS_BAND_UNROLL
+#define FS_BAND_UNROLL 2
+#endif
+#ifndef FS_BAND_ACC2
+#define FS_BAND_ACC2 0
+#endif
+constexpr int kBandUnroll = FS_BAND_UNROLL;
 constexpr bool kStage64 = FS_STAGE64;
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
@@ -359,7 +367,26 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             double T[kR];
 #pragma unroll
             for (int r = 0; r < kR; ++r) T[r] = (jend <= J[r]) ? tl[r] : tl[r] + L;  // the tile's image
-#pragma unroll 2
+#if FS_BAND_ACC2
+            // two accumulators per target (even and odd sources): half the
+            // loop-carried FMA chain
+            double accb[kR];
+#pragma unroll
+            for (int r = 0; r < kR; ++r) accb[r] = 0.0;
+#pragma unroll 1
+            for (int j = 0; j < kS; j += 2) {
+                const double2 e0 = tile64[j], e1 = tile64[j + 1];
+#pragma unroll
+                for (int r = 0; r < kR; ++r) {
+                    const double d0 = T[r] - e0.x, d1 = T[r] - e1.x;
+                    acc64[r] = fma(e0.y * d0, rsqrt_nr64(fma(d0, d0, e2d)), acc64[r]);
+                    accb[r] = fma(e1.y * d1, rsqrt_nr64(fma(d1, d1, e2d)), accb[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kR; ++r) acc64[r] += accb[r];
+#else
+#pragma unroll(kBandUnroll)
             for (int j = 0; j < kS; ++j) {
                 const double2 e = tile64[j];
 #pragma unroll
@@ -368,6 +395,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                     acc64[r] = fma(e.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
                 }
             }
+#endif
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
             // two targets per packed FP32x2 op, one MUFU.RCP per two targets
