@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import multi_species_b200 as fs
+from field_error import fp32c_bound
 from multi_species_b200 import decks
 
 pytestmark = pytest.mark.gpu
@@ -79,12 +80,17 @@ def test_autotuned_pool_matches_alone_within_tolerance():
         sim.close()
         # decks without cold ions: the remesh at step 5 locates every point in
         # the same panel alone and in the mix, so the run stays within 1e-6
-        for k in ("es", "fs", "xs"):
-            assert _rel(got[k], ref[k]) <= 1e-6, k
+        # (E within the field's stated error model: 1e-6 relative, or 2e-9 of
+        # the band-charge scale for a field caught near a node)
         L = d["xmax"] - d["xmin"]
         f = fs.E_MQ_DirectSum_B200(L, d["greens_epsilon"], "fp64")
-        assert _rel(got["es"], f.evaluate(got["xs"], got["xs"], got["q_ws"])) <= 1e-6
+        e64 = f.evaluate(got["xs"], got["xs"], got["q_ws"])
         f.close()
+        tol = fp32c_bound(got["xs"], got["q_ws"], L, d["greens_epsilon"], e64)
+        for k in ("fs", "xs"):
+            assert _rel(got[k], ref[k]) <= 1e-6, k
+        assert np.linalg.norm(got["es"] - ref["es"]) <= tol
+        assert np.linalg.norm(got["es"] - e64) <= tol
     pool.close()
 
 
