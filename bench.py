@@ -288,6 +288,20 @@ def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
             "pairs_per_launch": kwork / kl if kl else None,
             "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
             "kernel_share_of_step_time": kms / total_ms if total_ms else None}
+    if a.field == "direct32c" and kern == "k_pairs32":
+        # far pairs on the FP32 pipe and MUFU, band pairs (|d| <= 16 eps) on
+        # the FP64 pipe: the kernel's bound is the time of both at their peaks
+        import multi_species_b200 as M
+        band = M.profile_read("pairs32_band_pairs")[2]
+        if band > 0 and kms > 0:
+            fp64_band_peak = sm * FP64_LANES_PER_CLK_PER_SM * clk_hz / BAND64_FP64_INSTR_PER_PAIR
+            t_bound = (kwork - band) / fp32_peak + band / fp64_band_peak
+            roof.update({"bound": "fp32-pipe (far pairs) + fp64-pipe (band pairs)",
+                         "frac": t_bound / (kms / 1e3), "band_pairs_per_launch": band / kl,
+                         "band_fraction": band / kwork, "fp64_band_peak_gpairs": fp64_band_peak / 1e9,
+                         "frac_note": "frac = (far pairs / FP32-pipe peak + band pairs / FP64-pipe peak) / kernel "
+                                      "time; achieved and peak are the direct-equivalent rate against the FP32 "
+                                      "bound alone"})
     if a.field == "direct64":
         # two IEEE divisions + one square root + ~11 FP64 ops per pair, no MUFU shortcut
         roof.update({"bound": "fp64-pipe", "peak": None, "frac": None, "mufu_convention": None,
@@ -413,6 +427,10 @@ FP64_LANES_PER_CLK_PER_SM = 64
 # over the launch's pairs) on the two-stream deck at 33,153 points; the count
 # per pair does not depend on the size.
 DIRECT64_FP64_INSTR_PER_PAIR = 40.2
+# FP64 instructions per band pair of k_pairs32: d (DADD), d^2 + eps^2 (DFMA),
+# the Newton step on the hardware 1/sqrt (DMUL, DMUL, DFMA, DMUL) and
+# q/2 d y accumulated (DMUL, DFMA); plus one MUFU op.
+BAND64_FP64_INSTR_PER_PAIR = 8.0
 
 
 def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):

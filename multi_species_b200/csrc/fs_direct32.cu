@@ -245,7 +245,7 @@ static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "f
 #endif
 // band tiles: sources per unrolled body, and two accumulators per target (1)
 #ifndef FS_BAND_UNROLL
-#define FS_BAND_UNROLL 2
+#define FS_BAND_UNROLL 4
 #endif
 #ifndef FS_BAND_ACC2
 #define FS_BAND_ACC2 0
@@ -641,6 +641,22 @@ __global__ void k_finalize32(const double* __restrict__ partial, int nchunks, in
     apply_stage(S, tperm[i], E);
 }
 
+// Band pairs of an evaluation (sum over targets of U2 - U1), for the
+// profile's roofline: they run on the FP64 pipe, the far pairs on FP32/MUFU.
+__global__ void k_band_count(int nt, const TargetInfo* __restrict__ info, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double c = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += gridDim.x * blockDim.x)
+        c += (double)(info[i].U2 - info[i].U1);
+    sh[threadIdx.x] = c;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(out, sh[0]);
+}
+
 class Direct32c final : public FieldEngine {
    public:
     Direct32c(double L, double eps) : L_(L), eps_(eps) {
@@ -677,6 +693,7 @@ class Direct32c final : public FieldEngine {
     bool prepare(const double* d_t, int nt, const double* d_s, const double* d_q, int ns, const Stage& stage,
                  cudaStream_t st, int tpc, PairJob* job) override {
         last_pairs = (double)nt * (double)ns;
+        last_nt_ = 0;
         fin_ = Fin{};
         if (nt <= 0) return false;
         const bool same = (d_t == d_s) && (nt == ns);
@@ -724,6 +741,7 @@ class Direct32c final : public FieldEngine {
         k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(tkeys, nt, nt_pad, kout_.p, ns, L_, kBand * eps_, pq_.p,
                                                          info_.p);
         FS_LAUNCHED(1);
+        last_nt_ = nt;
         *job = PairJob{src_.p, src64_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
                        (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
         return true;
@@ -739,6 +757,20 @@ class Direct32c final : public FieldEngine {
     }
 
     int* error_flag() override { return err_.p; }
+
+    // Pairs of the last evaluation (each evaluated); while profiling, also the
+    // band pairs among them, recorded as "pairs32_band_pairs".
+    double actual_work(cudaStream_t st) override {
+        if (last_pairs <= 0 || last_nt_ <= 0) return last_pairs;
+        FS_CUDA(cudaMemsetAsync(bandcount_.p, 0, sizeof(double), st));
+        k_band_count<<<148, 256, 0, st>>>(last_nt_, info_.p, bandcount_.p);
+        FS_LAUNCHED(1);
+        double h = 0.0;
+        FS_CUDA(cudaMemcpyAsync(&h, bandcount_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+        FS_CUDA(cudaStreamSynchronize(st));
+        prof_add_work("pairs32_band_pairs", h);
+        return last_pairs;
+    }
 
    private:
     void reserve(int ns, int ns_pad, int nt_sep, int nt_pad, size_t npartial, int ntiles) {
@@ -759,6 +791,7 @@ class Direct32c final : public FieldEngine {
             err_.ensure(1);
             FS_CUDA(cudaMemset(err_.p, 0, sizeof(int)));
             counter_.ensure(1);
+            bandcount_.ensure(1);
         }
         const int nsort = std::max(ns, nt_sep);
         if (nt_sep) {
@@ -792,6 +825,8 @@ class Direct32c final : public FieldEngine {
     DevBuf<int> iin_, iout_, tiin_, tiout_;
     DevBuf<float4> src_;
     DevBuf<double2> src64_;
+    DevBuf<double> bandcount_;
+    int last_nt_ = 0;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
