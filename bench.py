@@ -410,8 +410,8 @@ def run_ours(a, rank, world, local_rank):
 VALUE_NOTE = {
     "direct32c": "pairs are direct-equivalent: N^2 per full evaluation (and U^2 per reduced-grid evaluation) at the "
                  "accuracy stated in `accuracy`; far pairs (|d| > 16 eps) are summed as an exact FP64 sign part plus a "
-                 "one-term series of analytic error <= v^2/16 (v = eps^2/(d^2+eps^2)), band pairs exactly in FP32 with "
-                 "compensation",
+                 "one-term series of analytic error <= v^2/16 (v = eps^2/(d^2+eps^2)) accumulated in FP32, band pairs "
+                 "(|d| <= 16 eps) in FP64",
     "direct64": "pairs evaluated one by one with the reference's FP64 arithmetic (bit-identical)",
     "treecode32c": "pairs are direct-equivalent N^2 per evaluation; the treecode evaluates near-field pairs and "
                    "far-field cluster terms (kernel_evals_per_s)",

@@ -93,7 +93,8 @@ fs_status fs_field_eval_device(fs_field* field, double* d_es, const double* d_ta
  * array of about 9.5 MiB that each GPU loading the library keeps until exit;
  * n is limited to 32768 (larger n returns FS_ERR_ARG).  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) for that
- * device; make that first call before any stream capture.  Calls share the
+ * device.  The call waits for its own work: it returns after d_es is written
+ * (or the error is known).  Calls share the
  * array, so calls that overlap on one GPU race: serialise them.  The looked-up
  * address is kept for the life of the process; after cudaDeviceReset on a
  * device, reload the library before calling this again there.  When the call

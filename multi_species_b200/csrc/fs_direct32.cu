@@ -16,23 +16,26 @@
 //    (sources before / after J_i take one of two images); the FP64 background
 //    term uses the same split, so both halves of the kernel agree exactly on
 //    which image a pair uses.
-//  * Per target the sources split into a far band (|d| > 24 eps) and a near
-//    band, by index (binary searches in FP64).  A far pair contributes
-//    sign(d) q/2 (1 - c(v)) with v = eps^2/(d^2+eps^2) <= 1/577: the sign(d) q/2
-//    part is summed exactly in FP64 from prefix sums of the FP64 charges; the
-//    pair kernel only accumulates q/2 * c(v), c = v/2 + v^2/8 (series of
-//    1-sqrt(1-v)), which is O(eps^2/d^2) and carries FP32's relative error on
-//    a small quantity.  Near-band pairs (|d| <= 24 eps, a few percent) use the
-//    full q/2 d*y with Kahan-compensated FP32 accumulation.  Every tile's
-//    partial sum is added into an FP64 accumulator.
-//  * Far pairs need no square root: per two targets, FADD2, FFMA2 (d, d^2+eps^2
-//    packed), one FMUL + one MUFU.RCP for both reciprocals, FMUL2, FFMA2,
-//    FMUL2, FFMA2 -- 6.5 FP32 lane-operations and 0.5 MUFU op per pair, so
-//    the FP32 datapath (128 lanes/clk/SM), not the MUFU pipe, bounds it; source tiles
-//    moved global->shared by TMA bulk copies (cp.async.bulk, no multicast)
+//  * Per target the sources split into far pairs (|d| > 16 eps) and a band
+//    (|d| <= 16 eps), by index (binary searches in FP64).  A far pair
+//    contributes sign(d) q/2 (1 - c(v)) with v = eps^2/(d^2+eps^2) <= 1/257:
+//    the sign(d) q/2 part is summed exactly in FP64 from prefix sums of the
+//    FP64 charges; the pair kernel only accumulates q/2 * c(v) in FP32, with
+//    the shifted one-term series c = a1 / (d^2 + 3 eps^2 / 4), a1 = eps^2/2,
+//    whose error is below v^2/16 of c and which carries FP32's relative error
+//    on a quantity of order eps^2/d^2.  Band pairs (about 2% on the two-stream
+//    deck) are evaluated in FP64, q/2 d / sqrt(d^2 + eps^2), from FP64 source
+//    records staged beside the FP32 ones.  Every tile's partial sum is added
+//    into an FP64 accumulator.
+//  * Far pairs need no square root: per two targets FFMA2 (d), FFMA2
+//    (d^2 + 3 eps^2/4), FMUL + one MUFU.RCP for both reciprocals, FMUL, FFMA2:
+//    4 FP32 lane-operations and 0.5 MUFU op per pair, loading the FP32
+//    datapath (128 lanes/clk/SM) and MUFU (16/clk/SM) equally.  Source tiles
+//    move global->shared by TMA bulk copies (cp.async.bulk, no multicast),
 //    double-buffered on mbarriers.
 //
-// Work is split over (target block, source chunk) CTAs; chunk partials are
+// Work is split into (target block, source chunk) items, taken from an atomic
+// counter by a one-wave persistent grid, heaviest first; chunk partials are
 // summed in a fixed order by the finalize kernel, which also applies the fused
 // RK4 stage epilogue.
 #include <cub/cub.cuh>
@@ -106,23 +109,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 __device__ __forceinline__ double key_to_x(uint64_t k) { return __longlong_as_double((long long)k); }
 
-// 1/sqrt(r) in FP64 for r > 0: the hardware approximation refined by one
-// Newton-Raphson step y (3/2 - r y^2 / 2), which squares its relative error.
-#ifndef FS_RSQ_SEED32
-#define FS_RSQ_SEED32 0
-#endif
-__device__ __forceinline__ double rsqrt_nr64(double r) {
+// Band pair in FP64, accumulated: acc + (q/2) d / sqrt(r), r = d^2 + eps^2,
+// from the source's q/4.  1/sqrt(r) is the hardware approximation y refined
+// by one Newton-Raphson step y (3 - r y^2) / 2 (which squares its relative
+// error); the step's 1/2 is folded into the stored q/4:
+//   (q/2) d y (3 - r y^2) / 2 = ((q/4) d y) (3 - r y^2),
+// 7 FP64 operations per pair with the difference and r.
+__device__ __forceinline__ double band_acc64(double q4, double d, double r, double acc) {
     double y;
-    if (FS_RSQ_SEED32) {
-        // seed from the FP32 approximation (relative error below 2^-22 for the
-        // band's r in [eps^2, 257 eps^2], well inside FP32's range)
-        y = (double)rsqrt_approx((float)r);
-    } else {
-        asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
-    }
-    const double t = y * y;
-    const double u = fma(-0.5 * r, t, 1.5);
-    return y * u;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
+    const double a = (q4 * d) * y;
+    const double v = fma(-r, y * y, 3.0);
+    return fma(a, v, acc);
 }
 
 // x -> [0, L) and its order-preserving key (non-negative doubles sort as
@@ -160,7 +158,7 @@ __global__ void k_gather_sources(const uint64_t* __restrict__ skeys, const int* 
     const double qj = q[sidx[j]];
     const float qh = (float)(0.5 * qj);
     src[j] = make_float4((float)(xj - base), qh, (float)((double)qh * a1), (float)((double)qh * a2));
-    src64[j] = make_double2(xj, 0.5 * qj);
+    src64[j] = make_double2(xj, 0.25 * qj);
     qs[j] = qj;
     qx[j] = qj * xj;
 }
@@ -243,14 +241,16 @@ static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "f
 #ifndef FS_STAGE64
 #define FS_STAGE64 1
 #endif
-// band tiles: sources per unrolled body, and two accumulators per target (1)
+// band tiles: sources per unrolled body
 #ifndef FS_BAND_UNROLL
 #define FS_BAND_UNROLL 4
 #endif
-#ifndef FS_BAND_ACC2
-#define FS_BAND_ACC2 0
-#endif
 constexpr int kBandUnroll = FS_BAND_UNROLL;
+// far tiles: warps of a CTA (of four) that use one reciprocal per four targets
+#ifndef FS_QUAD_WARPS
+#define FS_QUAD_WARPS 0
+#endif
+constexpr int kQuadWarps = FS_QUAD_WARPS;
 constexpr bool kStage64 = FS_STAGE64;
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
@@ -367,35 +367,15 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             double T[kR];
 #pragma unroll
             for (int r = 0; r < kR; ++r) T[r] = (jend <= J[r]) ? tl[r] : tl[r] + L;  // the tile's image
-#if FS_BAND_ACC2
-            // two accumulators per target (even and odd sources): half the
-            // loop-carried FMA chain
-            double accb[kR];
-#pragma unroll
-            for (int r = 0; r < kR; ++r) accb[r] = 0.0;
-#pragma unroll 1
-            for (int j = 0; j < kS; j += 2) {
-                const double2 e0 = tile64[j], e1 = tile64[j + 1];
-#pragma unroll
-                for (int r = 0; r < kR; ++r) {
-                    const double d0 = T[r] - e0.x, d1 = T[r] - e1.x;
-                    acc64[r] = fma(e0.y * d0, rsqrt_nr64(fma(d0, d0, e2d)), acc64[r]);
-                    accb[r] = fma(e1.y * d1, rsqrt_nr64(fma(d1, d1, e2d)), accb[r]);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kR; ++r) acc64[r] += accb[r];
-#else
 #pragma unroll(kBandUnroll)
             for (int j = 0; j < kS; ++j) {
                 const double2 e = tile64[j];
 #pragma unroll
                 for (int r = 0; r < kR; ++r) {
                     const double d = T[r] - e.x;
-                    acc64[r] = fma(e.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
+                    acc64[r] = band_acc64(e.y, d, fma(d, d, e2d), acc64[r]);
                 }
             }
-#endif
         } else if (!__any_sync(0xffffffffu, careful)) {
             // far tiles: accumulate q/2 * c(v) = (q/2 a1) w', w' = 1/(d^2 + 3 eps^2/4),
             // two targets per packed FP32x2 op, one MUFU.RCP per two targets
@@ -415,20 +395,47 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             // sources measured 0.5-3.7% slower.)  The FP32 sums are moved into
             // the FP64 accumulators every kFarChunk sources.
             constexpr int kChunk = kFarChunk ? kFarChunk : kS;
+            // warps below kQuadWarps share one reciprocal between four targets
+            // (4.5 lane-ops, 0.25 MUFU per pair), the others between two, so
+            // that the SM's warps load the FMA pipe and MUFU unequally
+            const bool quad = (kR >= 4) && ((int)(threadIdx.x >> 5) < kQuadWarps);
 #pragma unroll 1
             for (int c = 0; c < kS; c += kChunk) {
+                if (quad) {
 #pragma unroll 1
-                for (int j0 = c; j0 < c + kChunk; j0 += 8) {
+                    for (int j0 = c; j0 < c + kChunk; j0 += 8) {
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const float4 e = tile[j0 + k];
-                        const float2 sx2 = make_float2(e.x, e.x);
+                        for (int k = 0; k < 8; ++k) {
+                            const float4 e = tile[j0 + k];
+                            const float2 sx2 = make_float2(e.x, e.x);
 #pragma unroll
-                        for (int h = 0; h < kR / 2; ++h) {
-                            const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
-                            const float2 r2 = __ffma2_rn(d, d, e2v);
-                            const float qW = e.z * rcp_approx(r2.x * r2.y);
-                            acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
+                            for (int g = 0; g < kR / 4; ++g) {
+                                const float2 d0 = __ffma2_rn(sx2, m1, tau2[2 * g]);
+                                const float2 d1 = __ffma2_rn(sx2, m1, tau2[2 * g + 1]);
+                                const float2 r0 = __ffma2_rn(d0, d0, e2v);
+                                const float2 r1 = __ffma2_rn(d1, d1, e2v);
+                                const float p0 = r0.x * r0.y, p1 = r1.x * r1.y;
+                                const float qW = e.z * rcp_approx(p0 * p1);
+                                const float w0 = qW * p1, w1 = qW * p0;
+                                acc2[2 * g] = __ffma2_rn(r0, make_float2(w0, w0), acc2[2 * g]);
+                                acc2[2 * g + 1] = __ffma2_rn(r1, make_float2(w1, w1), acc2[2 * g + 1]);
+                            }
+                        }
+                    }
+                } else {
+#pragma unroll 1
+                    for (int j0 = c; j0 < c + kChunk; j0 += 8) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const float4 e = tile[j0 + k];
+                            const float2 sx2 = make_float2(e.x, e.x);
+#pragma unroll
+                            for (int h = 0; h < kR / 2; ++h) {
+                                const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
+                                const float2 r2 = __ffma2_rn(d, d, e2v);
+                                const float qW = e.z * rcp_approx(r2.x * r2.y);
+                                acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
+                            }
                         }
                     }
                 }
@@ -460,7 +467,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                     if (u >= U1[r] && u < U2[r]) {
                         const double2 e64 = tile64[j];
                         const double d = (lo_img ? tl[r] : tl[r] + L) - e64.x;
-                        acc64[r] = fma(e64.y * d, rsqrt_nr64(fma(d, d, e2d)), acc64[r]);
+                        acc64[r] = band_acc64(e64.y, d, fma(d, d, e2d), acc64[r]);
                     } else {
                         const float d = (lo_img ? tau[r] : tauh[r]) - e.x;
                         const float y = rsqrt_approx(fmaf(d, d, eps2));
@@ -511,7 +518,8 @@ __global__ void __launch_bounds__(kNT) k_pairs32(PairJob job, int* __restrict__ 
 // ordered longest first.
 template <int kR>
 __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items,
-                                                         int nitems, int* __restrict__ counter, int* __restrict__ err) {
+                                                         int nitems, const int* __restrict__ order,
+                                                         int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
     __shared__ __align__(128) double2 buf64[2][kS];
     __shared__ __align__(8) uint64_t bar[2];
@@ -519,7 +527,10 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
     init_bars(bar);
     uint32_t gk = 0;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(counter, 1);
+            s_item = (order && k < nitems) ? order[k] : k;
+        }
         __syncthreads();
         const int item = s_item;
         __syncthreads();
@@ -531,10 +542,12 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
 }
 
 // One job, persistent: a grid of one wave of CTAs takes (chunk, target block)
-// items in chunk-major order from an atomic counter, so the last, shorter
-// chunk comes last and no SM idles through a partial final wave.
+// items from an atomic counter, in the order `order` gives (heaviest first,
+// chunk-major among equals, so the last, shorter chunk comes last) or in
+// chunk-major order when it is null.
 template <int kR>
 __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
+                                                            const int* __restrict__ order,
                                                             int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
     __shared__ __align__(128) double2 buf64[2][kS];
@@ -543,13 +556,84 @@ __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(Pai
     init_bars(bar);
     uint32_t gk = 0;
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        if (threadIdx.x == 0) {
+            const int k = atomicAdd(counter, 1);
+            s_item = (order && k < nitems) ? order[k] : k;
+        }
         __syncthreads();
         const int item = s_item;
         __syncthreads();
         if (item >= nitems) break;
         if (!pair_block<kR>(job, item % tblocks, item / tblocks, buf, buf64, bar, gk, err)) return;
     }
+}
+
+// Estimated cost of a (target block, source chunk) item: its tiles, plus
+// kNearTileCost - 1 more for every tile within the band of the block's
+// x-range (band and mixed tiles run the FP64 / per-pair paths, several times a
+// far tile's time).  Persistent launches take their items heaviest first, so
+// that they do not end on a band-heavy item.  Only the order of the items
+// depends on this; every item writes its own partial sums.
+constexpr int kNearTileCost = 4;
+#ifndef FS_ITEM_ORDER
+#define FS_ITEM_ORDER 1
+#endif
+constexpr bool kItemOrder = FS_ITEM_ORDER;
+constexpr int kCostBits = 24;  // costs are below 4 * tiles per chunk < 2^24
+
+__device__ __forceinline__ double target_x(const TargetInfo& T, double L) { return T.tlo < 0.0 ? T.tlo + L : T.tlo; }
+
+__device__ int item_cost(const PairJob& J, int tb, int c, int ttb) {
+    const int t0 = c * J.tpc, t1 = min(J.ntiles, t0 + J.tpc);
+    if (t0 >= t1 || J.nt <= 0) return 0;
+    // the block's real targets, sorted by x: the first and the last bound it
+    const int first = min(tb * ttb, J.nt - 1), last = min(tb * ttb + ttb, J.nt) - 1;
+    const double xa = target_x(J.info[first], J.L), xb = target_x(J.info[last], J.L);
+    const double band = kBand * sqrt(J.eps2d);
+    int near = 0;
+    for (int t = t0; t < t1; ++t) {
+        const double ya = J.tbase[t];
+        const double yb = (t + 1 < J.ntiles) ? J.tbase[t + 1] : J.L;
+        double gap = 1e300;
+        for (int k = -1; k <= 1; ++k) {
+            const double sh = k * J.L;
+            gap = fmin(gap, fmax(0.0, fmax(ya + sh - xb, xa - (yb + sh))));
+        }
+        near += (gap <= band);
+    }
+    return (t1 - t0) + (kNearTileCost - 1) * near;
+}
+
+// item i = chunk * tblocks + target block, as k_pairs32_persistent reads it
+__global__ void k_item_cost(PairJob J, int nitems, int tblocks, int ttb, int* __restrict__ cost,
+                            int* __restrict__ ids) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    cost[i] = item_cost(J, i % tblocks, i / tblocks, ttb);
+    ids[i] = i;
+}
+
+__global__ void k_item_cost_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
+                                    int ttb, int* __restrict__ cost, int* __restrict__ ids) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nitems) return;
+    const int4 it = items[i];
+    cost[i] = item_cost(jobs[it.x], it.y, it.z, ttb);
+    ids[i] = i;
+}
+
+// Bytes of CUB scratch for ordering n items.
+size_t item_order_tmp_bytes(int n) {
+    size_t b = 0;
+    FS_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, b, (const int*)nullptr, (int*)nullptr,
+                                                      (const int*)nullptr, (int*)nullptr, n, 0, kCostBits));
+    return std::max<size_t>(b, 1);
+}
+
+// cost and ids hold 2 n ints each; the order is written to ids + n.
+void sort_items(int n, int* cost, int* ids, void* tmp, size_t tmp_bytes, cudaStream_t st) {
+    FS_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, cost, cost + n, ids, ids + n, n, 0,
+                                                      kCostBits, st));
 }
 
 // Targets per thread of the pair kernel: 2, 4 or 8 (register use vs. reuse of
@@ -573,26 +657,41 @@ int persistent_grid(int R) {
 }
 
 void launch_pairs_persistent(int R, int grid, cudaStream_t st, const PairJob& job, int tblocks, int nitems,
-                             int* counter, int* err) {
+                             const int* order, int* counter, int* err) {
     FS_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
     switch (R) {
-        case 2: k_pairs32_persistent<2><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
-        case 8: k_pairs32_persistent<8><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
-        default: k_pairs32_persistent<4><<<grid, kNT, 0, st>>>(job, tblocks, nitems, counter, err); break;
+        case 2: k_pairs32_persistent<2><<<grid, kNT, 0, st>>>(job, tblocks, nitems, order, counter, err); break;
+        case 8: k_pairs32_persistent<8><<<grid, kNT, 0, st>>>(job, tblocks, nitems, order, counter, err); break;
+        default: k_pairs32_persistent<4><<<grid, kNT, 0, st>>>(job, tblocks, nitems, order, counter, err); break;
     }
 }
 
 }  // namespace
 
 void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs, const int4* items, int nitems,
-                          int* counter, int* err) {
+                          ItemOrder* ord, int* counter, int* err) {
+    const int* order = nullptr;
+    if (kItemOrder && ord && nitems > grid) {
+        const int T = 256;
+        k_item_cost_batched<<<(nitems + T - 1) / T, T, 0, st>>>(jobs, items, nitems, kNT * R, ord->cost.p,
+                                                                ord->ids.p);
+        FS_LAUNCHED(1);
+        sort_items(nitems, ord->cost.p, ord->ids.p, ord->tmp.p, ord->tmp.n, st);
+        order = ord->ids.p + nitems;
+    }
     FS_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
     switch (R) {
-        case 2: k_pairs32_batched<2><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
-        case 8: k_pairs32_batched<8><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
-        default: k_pairs32_batched<4><<<grid, kNT, 0, st>>>(jobs, items, nitems, counter, err); break;
+        case 2: k_pairs32_batched<2><<<grid, kNT, 0, st>>>(jobs, items, nitems, order, counter, err); break;
+        case 8: k_pairs32_batched<8><<<grid, kNT, 0, st>>>(jobs, items, nitems, order, counter, err); break;
+        default: k_pairs32_batched<4><<<grid, kNT, 0, st>>>(jobs, items, nitems, order, counter, err); break;
     }
     FS_LAUNCHED(1);
+}
+
+void ItemOrder::reserve(int nitems) {
+    cost.ensure(2 * (size_t)std::max(nitems, 1));
+    ids.ensure(2 * (size_t)std::max(nitems, 1));
+    tmp.ensure(item_order_tmp_bytes(std::max(nitems, 1)));
 }
 
 void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost) {
@@ -683,8 +782,10 @@ class Direct32c final : public FieldEngine {
         if (prepare(d_t, nt, d_s, d_q, ns, stage, st, tpc, &job)) {
             nchunks = (job.ntiles + job.tpc - 1) / job.tpc;
             const int nitems = tblocks * nchunks;
+            const int* order = kItemOrder && nitems > grid_ ? item_order(nitems, tblocks, job, st) : nullptr;
             ProfScope prof("k_pairs32", st, last_pairs);
-            launch_pairs_persistent(R_, std::min(grid_, nitems), st, job, tblocks, nitems, counter_.p, err_.p);
+            launch_pairs_persistent(R_, std::min(grid_, nitems), st, job, tblocks, nitems, order, counter_.p,
+                                    err_.p);
             FS_LAUNCHED(1);
         }
         finalize(st);
@@ -743,7 +844,7 @@ class Direct32c final : public FieldEngine {
         FS_LAUNCHED(1);
         last_nt_ = nt;
         *job = PairJob{src_.p, src64_.p, tbase_.p, info_.p, partial_.p, ns, ntiles, tpc, nt_pad, L_, (float)e2,
-                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
+                       (float)(e2 / 2), (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, nt};
         return true;
     }
 
@@ -773,6 +874,21 @@ class Direct32c final : public FieldEngine {
     }
 
    private:
+    // The persistent launch's items ordered by descending estimated cost
+    // (stable: equal costs keep chunk-major order, so the short last chunk
+    // comes last).
+    const int* item_order(int nitems, int tblocks, const PairJob& job, cudaStream_t st) {
+        cost_.ensure(2 * (size_t)nitems);
+        ids_.ensure(2 * (size_t)nitems);
+        const size_t tb = item_order_tmp_bytes(nitems);
+        ordtmp_.ensure(tb);
+        const int T = 256;
+        k_item_cost<<<(nitems + T - 1) / T, T, 0, st>>>(job, nitems, tblocks, job.nt_pad / tblocks, cost_.p, ids_.p);
+        FS_LAUNCHED(1);
+        sort_items(nitems, cost_.p, ids_.p, ordtmp_.p, tb, st);
+        return ids_.p + nitems;
+    }
+
     void reserve(int ns, int ns_pad, int nt_sep, int nt_pad, size_t npartial, int ntiles) {
         kin_.ensure(ns);
         kout_.ensure(ns);
@@ -827,6 +943,8 @@ class Direct32c final : public FieldEngine {
     DevBuf<double2> src64_;
     DevBuf<double> bandcount_;
     int last_nt_ = 0;
+    DevBuf<int> cost_, ids_;
+    DevBuf<unsigned char> ordtmp_;
     DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
@@ -989,7 +1107,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
     const PairJob job{src, src64, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
-                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2};
+                      (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, n};
     launch_pairs(R, dim3(tblocks, nchunks), st, job, err);
     Stage S;
     S.kind = STAGE_STORE;

@@ -193,7 +193,7 @@ struct TargetInfo {
 // One field evaluation's FP32 pair work, as the pair kernels see it.
 struct PairJob {
     const float4* src;        // tile-relative source records {s, q/2, q/2 a1, q/2 a2}
-    const double2* src64;     // the same sources in FP64: {x (wrapped), q/2}, for band pairs
+    const double2* src64;     // the same sources in FP64: {x (wrapped), q/4}, for band pairs
     const double* tbase;      // FP64 tile bases
     const TargetInfo* info;   // per sorted target (nt_pad entries)
     double* partial;          // chunks * nt_pad
@@ -202,6 +202,7 @@ struct PairJob {
     float eps2, a1, a2;  // near band: eps^2, eps^2/2, eps^4/8
     float e2f;           // far pairs: 3 eps^2 / 4
     double eps2d;        // band pairs (FP64): eps^2
+    int nt;              // targets: the first nt of the nt_pad entries of info are real
 };
 
 class FieldEngine {
@@ -242,10 +243,20 @@ class FieldEngine {
 // message for fs_last_error().
 fs_status guard(const std::function<void()>& fn);
 
+// Device scratch for ordering the items of a batched launch by their
+// estimated cost (reserve() before any graph capture; it may allocate).
+struct ItemOrder {
+    DevBuf<int> cost, ids;
+    DevBuf<unsigned char> tmp;
+    void reserve(int nitems);
+};
+
 // Batched FP32 pair work (csrc/fs_direct32.cu): one persistent launch over the
-// (job, target block, source chunk) items of many field evaluations.
+// (job, target block, source chunk) items of many field evaluations, taken
+// heaviest first by the device's cost estimate when `ord` is given (reserved
+// for at least nitems).
 void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs, const int4* items, int nitems,
-                          int* counter, int* err);
+                          ItemOrder* ord, int* counter, int* err);
 int pairs_batched_grid(int R);
 // Items of one job for R targets per thread (target blocks x chunks) and the
 // work of each (tiles x targets), appended to `items` / `cost`.

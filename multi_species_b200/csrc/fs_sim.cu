@@ -1977,6 +1977,7 @@ struct Batch {
     int R = 4, tpc = 32;
     bool tuned = false;
     DevBuf<int> counter, err;
+    ItemOrder order;  // device cost order of the batched launch's items
     // slots and graphs are keyed by the step's remesh mask (one char per member)
     std::map<std::string, std::array<Slot, 4>> slots;
     std::map<std::string, Graph> graphs;
@@ -2079,8 +2080,8 @@ struct Batch {
         nitems = (int)items.size();
         std::vector<unsigned char> bytes(sizeof(PairJob) * jobs.size() + sizeof(int4) * items.size());
         std::memcpy(bytes.data(), jobs.data(), sizeof(PairJob) * jobs.size());
-        // the item block starts at 72 * jobs bytes: not 16-byte aligned for an
-        // odd job count, so copy bytewise rather than through an int4 pointer
+        // the item block starts after the jobs, which need not leave it
+        // 16-byte aligned, so copy bytewise rather than through an int4 pointer
         unsigned char* dst = bytes.data() + sizeof(PairJob) * jobs.size();
         for (size_t i = 0; i < order.size(); ++i) std::memcpy(dst + i * sizeof(int4), &items[order[i]], sizeof(int4));
         return bytes;
@@ -2094,6 +2095,7 @@ struct Batch {
         if (capturing) throw Capturing{};
         sl.jobs.ensure(jobs.size());
         sl.items.ensure(std::max(nitems, 1));
+        order.reserve(nitems);
         FS_CUDA(cudaMemcpyAsync(sl.jobs.p, bytes.data(), sizeof(PairJob) * jobs.size(), cudaMemcpyHostToDevice, st));
         FS_CUDA(cudaMemcpyAsync(sl.items.p, bytes.data() + sizeof(PairJob) * jobs.size(), sizeof(int4) * nitems,
                                 cudaMemcpyHostToDevice, st));
@@ -2104,7 +2106,8 @@ struct Batch {
     }
 
     void launch(const Slot& sl, int R_) {
-        launch_pairs_batched(R_, pairs_batched_grid(R_), st, sl.jobs.p, sl.items.p, sl.nitems, counter.p, err.p);
+        launch_pairs_batched(R_, pairs_batched_grid(R_), st, sl.jobs.p, sl.items.p, sl.nitems, &order, counter.p,
+                             err.p);
     }
 
     static bool joins(const Sim& s) { return s.prm.field_kind == FS_FIELD_DIRECT32C; }
