@@ -428,9 +428,9 @@ FP64_LANES_PER_CLK_PER_SM = 64
 # per pair does not depend on the size.
 DIRECT64_FP64_INSTR_PER_PAIR = 40.2
 # FP64 instructions per band pair of k_pairs32: d (DADD), d^2 + eps^2 (DFMA),
-# the Newton step on the hardware 1/sqrt (DMUL, DMUL, DFMA, DMUL) and
-# q/2 d y accumulated (DMUL, DFMA); plus one MUFU op.
-BAND64_FP64_INSTR_PER_PAIR = 8.0
+# (q/4) d y (two DMUL), y^2 (DMUL), 3 - r y^2 (DFMA) and the accumulation
+# (DFMA), the Newton step's 1/2 folded into q/4; plus one MUFU op.
+BAND64_FP64_INSTR_PER_PAIR = 7.0
 
 
 def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):

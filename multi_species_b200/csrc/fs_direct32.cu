@@ -35,7 +35,8 @@
 //    double-buffered on mbarriers.
 //
 // Work is split into (target block, source chunk) items, taken from an atomic
-// counter by a one-wave persistent grid, heaviest first; chunk partials are
+// counter by a one-wave persistent grid in an order estimated on the device
+// (band-heavy items spread over the queue, light ones last); chunk partials are
 // summed in a fixed order by the finalize kernel, which also applies the fused
 // RK4 stage epilogue.
 #include <cub/cub.cuh>
@@ -246,11 +247,12 @@ static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "f
 #define FS_BAND_UNROLL 4
 #endif
 constexpr int kBandUnroll = FS_BAND_UNROLL;
-// far tiles: warps of a CTA (of four) that use one reciprocal per four targets
-#ifndef FS_QUAD_WARPS
-#define FS_QUAD_WARPS 0
+// targets assigned contiguously per warp (1) or interleaved across the CTA (0)
+#ifndef FS_WARP_CONTIG
+#define FS_WARP_CONTIG 1
 #endif
-constexpr int kQuadWarps = FS_QUAD_WARPS;
+constexpr bool kWarpContig = FS_WARP_CONTIG;
+constexpr int kTStride = kWarpContig ? 32 : kNT;
 constexpr bool kStage64 = FS_STAGE64;
 
 // Far pairs: q/2 * d*y = sign(d) * q/2 * (1 - c), c = 1 - sqrt(1 - v),
@@ -285,12 +287,16 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
     const float eps2 = Jb.eps2, a1 = Jb.a1, a2 = Jb.a2;
     const double L = Jb.L;
     const int ns = Jb.ns;
-    const int ibase = tb * kTB + tid;
+    // targets of this thread: ibase + r * kTStride.  Per warp (kTStride = 32)
+    // a warp's 32 kR targets are contiguous in x, so fewer of its tiles mix
+    // band and far pairs; per CTA (kTStride = kNT) they interleave with the
+    // other warps'.
+    const int ibase = kWarpContig ? tb * kTB + (tid >> 5) * (32 * kR) + (tid & 31) : tb * kTB + tid;
     double tl[kR], acc64[kR];
     int J[kR], U1[kR], U2[kR];
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-        const TargetInfo T = Jb.info[ibase + r * kNT];  // nt_pad is a multiple of kTB
+        const TargetInfo T = Jb.info[ibase + r * kTStride];  // nt_pad is a multiple of kTB
         tl[r] = T.tlo;
         J[r] = T.J;
         U1[r] = T.U1;
@@ -391,51 +397,25 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             // product: q/2 a1 / r_a = (q/2 a1 W) r_b with W = 1/(r_a r_b), i.e.
             // 4 FP32 lane-ops and 0.5 MUFU.RCP per pair, which load the FMA pipe
             // and MUFU equally.  (One reciprocal per four targets -- 4.5
-            // lane-ops and 0.25 MUFU per pair -- mixed in for 1/8 to 1/2 of the
-            // sources measured 0.5-3.7% slower.)  The FP32 sums are moved into
-            // the FP64 accumulators every kFarChunk sources.
+            // lane-ops and 0.25 MUFU per pair -- for 1/8 to 1/2 of the sources
+            // measured 0.5-3.7% slower, and for 1, 2 or all 4 of a CTA's warps
+            // 3-4% slower.)  The FP32 sums are moved into the FP64
+            // accumulators every kFarChunk sources.
             constexpr int kChunk = kFarChunk ? kFarChunk : kS;
-            // warps below kQuadWarps share one reciprocal between four targets
-            // (4.5 lane-ops, 0.25 MUFU per pair), the others between two, so
-            // that the SM's warps load the FMA pipe and MUFU unequally
-            const bool quad = (kR >= 4) && ((int)(threadIdx.x >> 5) < kQuadWarps);
 #pragma unroll 1
             for (int c = 0; c < kS; c += kChunk) {
-                if (quad) {
 #pragma unroll 1
-                    for (int j0 = c; j0 < c + kChunk; j0 += 8) {
+                for (int j0 = c; j0 < c + kChunk; j0 += 8) {
 #pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const float4 e = tile[j0 + k];
-                            const float2 sx2 = make_float2(e.x, e.x);
+                    for (int k = 0; k < 8; ++k) {
+                        const float4 e = tile[j0 + k];
+                        const float2 sx2 = make_float2(e.x, e.x);
 #pragma unroll
-                            for (int g = 0; g < kR / 4; ++g) {
-                                const float2 d0 = __ffma2_rn(sx2, m1, tau2[2 * g]);
-                                const float2 d1 = __ffma2_rn(sx2, m1, tau2[2 * g + 1]);
-                                const float2 r0 = __ffma2_rn(d0, d0, e2v);
-                                const float2 r1 = __ffma2_rn(d1, d1, e2v);
-                                const float p0 = r0.x * r0.y, p1 = r1.x * r1.y;
-                                const float qW = e.z * rcp_approx(p0 * p1);
-                                const float w0 = qW * p1, w1 = qW * p0;
-                                acc2[2 * g] = __ffma2_rn(r0, make_float2(w0, w0), acc2[2 * g]);
-                                acc2[2 * g + 1] = __ffma2_rn(r1, make_float2(w1, w1), acc2[2 * g + 1]);
-                            }
-                        }
-                    }
-                } else {
-#pragma unroll 1
-                    for (int j0 = c; j0 < c + kChunk; j0 += 8) {
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const float4 e = tile[j0 + k];
-                            const float2 sx2 = make_float2(e.x, e.x);
-#pragma unroll
-                            for (int h = 0; h < kR / 2; ++h) {
-                                const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
-                                const float2 r2 = __ffma2_rn(d, d, e2v);
-                                const float qW = e.z * rcp_approx(r2.x * r2.y);
-                                acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
-                            }
+                        for (int h = 0; h < kR / 2; ++h) {
+                            const float2 d = __ffma2_rn(sx2, m1, tau2[h]);  // tau - s, exact product by -1
+                            const float2 r2 = __ffma2_rn(d, d, e2v);
+                            const float qW = e.z * rcp_approx(r2.x * r2.y);
+                            acc2[h] = __ffma2_rn(r2, make_float2(qW, qW), acc2[h]);
                         }
                     }
                 }
@@ -488,7 +468,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
     }
     double* out = Jb.partial + (size_t)chunk * Jb.nt_pad;
 #pragma unroll
-    for (int r = 0; r < kR; ++r) out[ibase + r * kNT] = acc64[r];
+    for (int r = 0; r < kR; ++r) out[ibase + r * kTStride] = acc64[r];
     return true;
 }
 
@@ -542,9 +522,9 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
 }
 
 // One job, persistent: a grid of one wave of CTAs takes (chunk, target block)
-// items from an atomic counter, in the order `order` gives (heaviest first,
-// chunk-major among equals, so the last, shorter chunk comes last) or in
-// chunk-major order when it is null.
+// items from an atomic counter, in the order `order` gives (band-heavy items
+// spread over the queue, light ones last) or in chunk-major order when it is
+// null.
 template <int kR>
 __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
                                                             const int* __restrict__ order,
@@ -571,19 +551,29 @@ __global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(Pai
 // Estimated cost of a (target block, source chunk) item: its tiles, plus
 // kNearTileCost - 1 more for every tile within the band of the block's
 // x-range (band and mixed tiles run the FP64 / per-pair paths, several times a
-// far tile's time).  Persistent launches take their items heaviest first, so
-// that they do not end on a band-heavy item.  Only the order of the items
-// depends on this; every item writes its own partial sums.
+// far tile's time).  Items with such tiles ("heavy") are spread evenly over
+// the launch's queue, heaviest first, with light items in the gaps and alone
+// in the last two waves: the launch does not end on a heavy item, and heavy
+// items' FP64 work runs beside other items' FP32 work on the same SMs rather
+// than all at once.  Only the order of the items depends on this; every item
+// writes its own partial sums.
 constexpr int kNearTileCost = 4;
 #ifndef FS_ITEM_ORDER
 #define FS_ITEM_ORDER 1
 #endif
 constexpr bool kItemOrder = FS_ITEM_ORDER;
-constexpr int kCostBits = 24;  // costs are below 4 * tiles per chunk < 2^24
+#ifndef FS_ITEM_SPREAD
+#define FS_ITEM_SPREAD 1
+#endif
+constexpr bool kItemSpread = FS_ITEM_SPREAD;
+constexpr int kCostBits = 24;           // sort keys: cost < 2^23, plus the heavy bit
+constexpr int kHeavy = 1 << 23;
 
 __device__ __forceinline__ double target_x(const TargetInfo& T, double L) { return T.tlo < 0.0 ? T.tlo + L : T.tlo; }
 
-__device__ int item_cost(const PairJob& J, int tb, int c, int ttb) {
+// Sort key of an item: its estimated cost, with kHeavy set when it has tiles
+// within the band; counts heavy items into *nheavy.
+__device__ int item_key(const PairJob& J, int tb, int c, int ttb, int* __restrict__ nheavy) {
     const int t0 = c * J.tpc, t1 = min(J.ntiles, t0 + J.tpc);
     if (t0 >= t1 || J.nt <= 0) return 0;
     // the block's real targets, sorted by x: the first and the last bound it
@@ -601,25 +591,48 @@ __device__ int item_cost(const PairJob& J, int tb, int c, int ttb) {
         }
         near += (gap <= band);
     }
-    return (t1 - t0) + (kNearTileCost - 1) * near;
+    const int cost = min((t1 - t0) + (kNearTileCost - 1) * near, kHeavy - 1);
+    if (near == 0) return cost;
+    atomicAdd(nheavy, 1);
+    return cost | kHeavy;
 }
 
 // item i = chunk * tblocks + target block, as k_pairs32_persistent reads it
-__global__ void k_item_cost(PairJob J, int nitems, int tblocks, int ttb, int* __restrict__ cost,
-                            int* __restrict__ ids) {
+__global__ void k_item_cost(PairJob J, int nitems, int tblocks, int ttb, int* __restrict__ key,
+                            int* __restrict__ ids, int* __restrict__ nheavy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
-    cost[i] = item_cost(J, i % tblocks, i / tblocks, ttb);
+    key[i] = item_key(J, i % tblocks, i / tblocks, ttb, nheavy);
     ids[i] = i;
 }
 
 __global__ void k_item_cost_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items, int nitems,
-                                    int ttb, int* __restrict__ cost, int* __restrict__ ids) {
+                                    int ttb, int* __restrict__ key, int* __restrict__ ids,
+                                    int* __restrict__ nheavy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
     const int4 it = items[i];
-    cost[i] = item_cost(jobs[it.x], it.y, it.z, ttb);
+    key[i] = item_key(jobs[it.x], it.y, it.z, ttb, nheavy);
     ids[i] = i;
+}
+
+// From the n items sorted by key (the H heavy ones first): heavy item j at
+// position floor(j span / H), span = n - guard, light items in the remaining
+// positions in their sorted order.  The heavy positions below p number
+// min(H, ceil(p H / span)).  With span < H there is nothing to spread: the
+// sorted order stands.
+__global__ void k_item_spread(const int* __restrict__ sorted, int n, const int* __restrict__ nheavy, int guard,
+                              int* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const long long H = *nheavy, span = n - guard;
+    if (H == 0 || span < H || !kItemSpread) {
+        out[p] = sorted[p];
+        return;
+    }
+    const long long below = min(H, (p * H + span - 1) / span);
+    const long long upto = min(H, ((p + 1) * H + span - 1) / span);
+    out[p] = (upto > below) ? sorted[below] : sorted[H + (p - below)];
 }
 
 // Bytes of CUB scratch for ordering n items.
@@ -630,10 +643,15 @@ size_t item_order_tmp_bytes(int n) {
     return std::max<size_t>(b, 1);
 }
 
-// cost and ids hold 2 n ints each; the order is written to ids + n.
-void sort_items(int n, int* cost, int* ids, void* tmp, size_t tmp_bytes, cudaStream_t st) {
-    FS_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, cost, cost + n, ids, ids + n, n, 0,
-                                                      kCostBits, st));
+// key holds 2 n + 1 ints (the heavy count last, already set), ids 3 n: the
+// sorted ids go to ids + n and the final order to ids + 2 n, which is returned.
+const int* order_items(int n, int* key, int* ids, int guard, void* tmp, size_t tmp_bytes, cudaStream_t st) {
+    FS_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, key, key + n, ids, ids + n, n, 0, kCostBits,
+                                                      st));
+    const int T = 256;
+    k_item_spread<<<(n + T - 1) / T, T, 0, st>>>(ids + n, n, key + 2 * n, guard, ids + 2 * n);
+    FS_LAUNCHED(1);
+    return ids + 2 * n;
 }
 
 // Targets per thread of the pair kernel: 2, 4 or 8 (register use vs. reuse of
@@ -673,11 +691,11 @@ void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs,
     const int* order = nullptr;
     if (kItemOrder && ord && nitems > grid) {
         const int T = 256;
+        FS_CUDA(cudaMemsetAsync(ord->cost.p + 2 * (size_t)nitems, 0, sizeof(int), st));
         k_item_cost_batched<<<(nitems + T - 1) / T, T, 0, st>>>(jobs, items, nitems, kNT * R, ord->cost.p,
-                                                                ord->ids.p);
+                                                                ord->ids.p, ord->cost.p + 2 * (size_t)nitems);
         FS_LAUNCHED(1);
-        sort_items(nitems, ord->cost.p, ord->ids.p, ord->tmp.p, ord->tmp.n, st);
-        order = ord->ids.p + nitems;
+        order = order_items(nitems, ord->cost.p, ord->ids.p, 2 * grid, ord->tmp.p, ord->tmp.n, st);
     }
     FS_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
     switch (R) {
@@ -689,8 +707,8 @@ void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs,
 }
 
 void ItemOrder::reserve(int nitems) {
-    cost.ensure(2 * (size_t)std::max(nitems, 1));
-    ids.ensure(2 * (size_t)std::max(nitems, 1));
+    cost.ensure(2 * (size_t)std::max(nitems, 1) + 1);
+    ids.ensure(3 * (size_t)std::max(nitems, 1));
     tmp.ensure(item_order_tmp_bytes(std::max(nitems, 1)));
 }
 
@@ -874,19 +892,19 @@ class Direct32c final : public FieldEngine {
     }
 
    private:
-    // The persistent launch's items ordered by descending estimated cost
-    // (stable: equal costs keep chunk-major order, so the short last chunk
-    // comes last).
+    // The persistent launch's items in the order of order_items (heavy items
+    // spread over the queue, light ones last).
     const int* item_order(int nitems, int tblocks, const PairJob& job, cudaStream_t st) {
-        cost_.ensure(2 * (size_t)nitems);
-        ids_.ensure(2 * (size_t)nitems);
+        cost_.ensure(2 * (size_t)nitems + 1);
+        ids_.ensure(3 * (size_t)nitems);
         const size_t tb = item_order_tmp_bytes(nitems);
         ordtmp_.ensure(tb);
         const int T = 256;
-        k_item_cost<<<(nitems + T - 1) / T, T, 0, st>>>(job, nitems, tblocks, job.nt_pad / tblocks, cost_.p, ids_.p);
+        FS_CUDA(cudaMemsetAsync(cost_.p + 2 * (size_t)nitems, 0, sizeof(int), st));
+        k_item_cost<<<(nitems + T - 1) / T, T, 0, st>>>(job, nitems, tblocks, job.nt_pad / tblocks, cost_.p, ids_.p,
+                                                        cost_.p + 2 * (size_t)nitems);
         FS_LAUNCHED(1);
-        sort_items(nitems, cost_.p, ids_.p, ordtmp_.p, tb, st);
-        return ids_.p + nitems;
+        return order_items(nitems, cost_.p, ids_.p, 2 * std::min(grid_, nitems), ordtmp_.p, tb, st);
     }
 
     void reserve(int ns, int ns_pad, int nt_sep, int nt_pad, size_t npartial, int ntiles) {

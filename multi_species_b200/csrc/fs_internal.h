@@ -252,9 +252,9 @@ struct ItemOrder {
 };
 
 // Batched FP32 pair work (csrc/fs_direct32.cu): one persistent launch over the
-// (job, target block, source chunk) items of many field evaluations, taken
-// heaviest first by the device's cost estimate when `ord` is given (reserved
-// for at least nitems).
+// (job, target block, source chunk) items of many field evaluations, in the
+// order of the device's cost estimate when `ord` is given (reserved for at
+// least nitems): band-heavy items spread over the queue, light ones last.
 void launch_pairs_batched(int R, int grid, cudaStream_t st, const PairJob* jobs, const int4* items, int nitems,
                           ItemOrder* ord, int* counter, int* err);
 int pairs_batched_grid(int R);
