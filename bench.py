@@ -440,9 +440,9 @@ def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):
       steps of an FP32c session and an FP64 session (W = 1/2 sum dx E^2 at the
       unique x in [0, L), the reference's diagnostic);
     * e_rel_l2 = ||E32 - E64|| / ||E64||: E32 the FP32c session's own field at
-      the end of its last step (a full evaluation, band arithmetic chosen by
-      the session as in the timed steps), E64 the plain FP64 sum on the same
-      positions and weights (all N targets and sources);
+      the end of its last step (a full evaluation, as in the timed steps), E64
+      the plain FP64 sum on the same positions and weights (all N targets and
+      sources);
     * plain_fp64_gpu: pair-interactions/s of the FP64 session (k_direct64, the
       reference arithmetic bit for bit; k_far_near64 for the treecode), CUDA
       events, with its kernel's FP64-pipe fraction."""
