@@ -269,8 +269,10 @@ KERNEL_OF_FIELD = {"direct32c": "k_pairs32", "direct64": "k_direct64", "treecode
                    "treecode64": "k_far_near64"}
 
 
-def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
-    """Roofline object for the dominant kernel of the field kind."""
+def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src, band_fraction=None):
+    """Roofline object for the dominant kernel of the field kind.  For the
+    FP32c pair kernels the band pairs (evaluated in FP64) come from the
+    profile (one simulation) or from `band_fraction` (a batch)."""
     mhz = float(peaks.get("sm_max_mhz", 1965.0))
     clk_hz = mhz * 1e6
     mufu_peak = sm * MUFU_PER_CLK_PER_SM * clk_hz        # one MUFU op per pair
@@ -288,11 +290,11 @@ def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src):
             "pairs_per_launch": kwork / kl if kl else None,
             "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
             "kernel_share_of_step_time": kms / total_ms if total_ms else None}
-    if a.field == "direct32c" and kern == "k_pairs32":
+    if a.field == "direct32c" and kern in ("k_pairs32", "k_pairs32_batched"):
         # far pairs on the FP32 pipe and MUFU, band pairs (|d| <= 16 eps) on
         # the FP64 pipe: the kernel's bound is the time of both at their peaks
         import multi_species_b200 as M
-        band = M.profile_read("pairs32_band_pairs")[2]
+        band = kwork * band_fraction if band_fraction is not None else M.profile_read("pairs32_band_pairs")[2]
         if band > 0 and kms > 0:
             fp64_band_peak = sm * FP64_LANES_PER_CLK_PER_SM * clk_hz / BAND64_FP64_INSTR_PER_PAIR
             t_bound = (kwork - band) / fp32_peak + band / fp64_band_peak
@@ -598,6 +600,7 @@ def run_batch(a, rank, world, local_rank):
     breakdown = {k: M.profile_read(k)[1] / a.steps for k in ("k_pairs32_batched", "batch_prepare", "batch_finalize",
                                                              "remesh")}
     stats = b.stats()
+    band, last = b.band_pairs()  # the last evaluation's band share stands for the timed ones
     b.close()
     total_ms = float(np.sum(step_ms))
     t_max = total_ms
@@ -618,7 +621,8 @@ def run_batch(a, rank, world, local_rank):
     peaks, peak_src = measured_peaks()
     sm = torch.cuda.get_device_properties(local_rank).multi_processor_count
     a.field = "direct32c"
-    roof = roofline(a, "k_pairs32_batched", kl, kms, kwork, total_ms, sm, peaks, peak_src)
+    roof = roofline(a, "k_pairs32_batched", kl, kms, kwork, total_ms, sm, peaks, peak_src,
+                    band_fraction=band / last if last > 0 else None)
     res = {"metric": "pair-interactions/s", "value": value, "unit": "pair-interactions/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t_max / a.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (deck-generated, no dataset)",

@@ -241,6 +241,11 @@ fs_status fs_batch_work(fs_batch* batch, double* pairs);
  * the number of steps replayed from graphs / run launch by launch. */
 fs_status fs_batch_stats(fs_batch* batch, int* targets_per_thread, int* tiles_per_item, long long* graph_steps,
                          long long* plain_steps);
+/* For the FP32-compensated members' last field evaluation (no counterpart in
+ * the reference): the pairs evaluated in FP64 (|d| <= 16 epsilon) and all
+ * pairs, so that a caller can bound the pair kernel by the FP32 pipe for the
+ * far pairs and the FP64 pipe for the band pairs.  Synchronises the batch. */
+fs_status fs_batch_band_pairs(fs_batch* batch, double* band_pairs, double* pairs);
 /* Fix the item shape instead of autotuning (targets per thread 4 or 8, source
  * tiles per item >= 1).  Pair sums are then made in the same order whatever
  * the other members are, so a member's results are bit-identical alone and in

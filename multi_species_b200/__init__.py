@@ -42,7 +42,7 @@ EXPORTS = ["fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eva
            "fs_mesh_fill", "fs_profile_enable", "fs_profile_read", "fs_profile_reset", "fs_last_error",
            "fs_version", "fs_kernel_launches", "fs_batch_create", "fs_batch_destroy", "fs_batch_add",
            "fs_batch_remove", "fs_batch_step", "fs_batch_export", "fs_batch_info", "fs_batch_step_times",
-           "fs_batch_work", "fs_batch_stats", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
+           "fs_batch_work", "fs_batch_stats", "fs_batch_band_pairs", "fs_batch_set_tuning", "fs_batch_set_graphs", "fs_pool_create",
            "fs_pool_destroy", "fs_pool_submit", "fs_pool_cancel", "fs_pool_poll", "fs_pool_wait", "fs_pool_result",
            "fs_pool_release", "fs_pool_step_times", "fs_pool_stats", "fs_pool_estimate_bytes", "fs_sim_set_output",
            "fs_sim_flush_output", "fs_sim_restart", "fs_initial_f0", "fs_debug_set_wait_limits"]
@@ -152,6 +152,7 @@ def lib():
         L.fs_batch_step_times.argtypes = [C.c_void_p, _dp, C.c_int, _ip]
         L.fs_batch_work.argtypes = [C.c_void_p, _dp]
         L.fs_batch_stats.argtypes = [C.c_void_p, _ip, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.fs_batch_band_pairs.argtypes = [C.c_void_p, _dp, _dp]
         L.fs_batch_set_graphs.argtypes = [C.c_void_p, C.c_int]
         L.fs_batch_set_tuning.argtypes = [C.c_void_p, C.c_int, C.c_int]
         _llp = C.POINTER(C.c_longlong)
@@ -172,7 +173,7 @@ def lib():
             getattr(L, n).restype = st
         for n in ("fs_batch_create", "fs_batch_destroy", "fs_batch_add", "fs_batch_remove", "fs_batch_step",
                   "fs_batch_export", "fs_batch_info", "fs_batch_step_times", "fs_batch_work", "fs_batch_stats",
-                  "fs_batch_set_tuning", "fs_batch_set_graphs"):
+                  "fs_batch_band_pairs", "fs_batch_set_tuning", "fs_batch_set_graphs"):
             getattr(L, n).restype = st
         for n in ("fs_field_create", "fs_field_destroy", "fs_field_eval", "fs_field_eval_device",
                   "fs_field_eval_noalloc", "fs_sim_create",
@@ -544,6 +545,13 @@ class Batch:
         _check(lib().fs_batch_stats(self._h, C.byref(r), C.byref(t), C.byref(g), C.byref(pl)))
         return {"targets_per_thread": r.value, "tiles_per_item": t.value, "graph_steps": g.value,
                 "plain_steps": pl.value}
+
+    def band_pairs(self) -> tuple:
+        """(band pairs, all pairs) of the FP32c members' last field evaluation:
+        the band pairs (|d| <= 16 eps) are the ones evaluated in FP64."""
+        b, a = C.c_double(), C.c_double()
+        _check(lib().fs_batch_band_pairs(self._h, C.byref(b), C.byref(a)))
+        return b.value, a.value
 
     def close(self) -> None:
         if getattr(self, "_h", None):

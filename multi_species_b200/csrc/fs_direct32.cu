@@ -54,7 +54,13 @@ namespace {
 #define FS_TILE_SOURCES 256
 #endif
 constexpr int kS = FS_TILE_SOURCES;  // sources per shared-memory tile
-constexpr int kNT = 128;         // threads per CTA
+// Threads per CTA: two warps (64) measured 1.3-1.5% faster than four (128)
+// on the two-stream and batch workloads (eight CTAs per SM instead of four, so
+// a CTA's barrier per tile holds fewer warps), one warp (32) no faster.
+#ifndef FS_NT
+#define FS_NT 64
+#endif
+constexpr int kNT = FS_NT;       // threads per CTA
 constexpr int kRMax = 8;         // largest number of targets per thread
 constexpr int kTBPad = kNT * kRMax;  // target counts are padded to a multiple of this
 
@@ -521,12 +527,20 @@ __global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restri
     }
 }
 
+// CTAs per SM (counted in 128-thread units) the 8-targets-per-thread
+// persistent kernel is compiled for: 3 (up to 168 registers per thread, 12
+// warps per SM) measured 0.9% faster than 4 (128 registers, 16 warps)
+#ifndef FS_MIN_BLOCKS8
+#define FS_MIN_BLOCKS8 3
+#endif
+constexpr int kMinBlocks8 = FS_MIN_BLOCKS8;
+
 // One job, persistent: a grid of one wave of CTAs takes (chunk, target block)
 // items from an atomic counter, in the order `order` gives (band-heavy items
 // spread over the queue, light ones last) or in chunk-major order when it is
 // null.
 template <int kR>
-__global__ void __launch_bounds__(kNT, kR >= 8 ? 4 : 8) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
+__global__ void __launch_bounds__(kNT, (kR >= 8 ? kMinBlocks8 : 8) * 128 / kNT) k_pairs32_persistent(PairJob job, int tblocks, int nitems,
                                                             const int* __restrict__ order,
                                                             int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
@@ -880,15 +894,19 @@ class Direct32c final : public FieldEngine {
     // Pairs of the last evaluation (each evaluated); while profiling, also the
     // band pairs among them, recorded as "pairs32_band_pairs".
     double actual_work(cudaStream_t st) override {
-        if (last_pairs <= 0 || last_nt_ <= 0) return last_pairs;
+        if (last_pairs > 0 && last_nt_ > 0) prof_add_work("pairs32_band_pairs", band_pairs(st));
+        return last_pairs;
+    }
+
+    double band_pairs(cudaStream_t st) override {
+        if (last_pairs <= 0 || last_nt_ <= 0) return 0.0;
         FS_CUDA(cudaMemsetAsync(bandcount_.p, 0, sizeof(double), st));
         k_band_count<<<148, 256, 0, st>>>(last_nt_, info_.p, bandcount_.p);
         FS_LAUNCHED(1);
         double h = 0.0;
         FS_CUDA(cudaMemcpyAsync(&h, bandcount_.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         FS_CUDA(cudaStreamSynchronize(st));
-        prof_add_work("pairs32_band_pairs", h);
-        return last_pairs;
+        return h;
     }
 
    private:

@@ -222,6 +222,12 @@ class FieldEngine {
         (void)st;
         return last_pairs;
     }
+    // Pairs of the last evaluation that the FP32c direct sum evaluates in FP64
+    // (|d| <= 16 eps); 0 for the other kinds.  Synchronises `st`.
+    virtual double band_pairs(cudaStream_t st) {
+        (void)st;
+        return 0.0;
+    }
     // Batched use.  prepare() runs everything before the pair kernel with
     // `tpc` source tiles per work chunk and fills *job, returning true; the
     // caller then runs the pair work (alone or batched with other jobs) and

@@ -2459,6 +2459,21 @@ fs_status fs_batch_work(fs_batch* b, double* pairs) {
     });
 }
 
+fs_status fs_batch_band_pairs(fs_batch* b, double* band_pairs, double* pairs) {
+    return fsb::guard([&] {
+        if (!b || !band_pairs || !pairs) fsb::fail(FS_ERR_ARG, "null argument");
+        FS_CUDA(cudaStreamSynchronize(b->impl.st));
+        double band = 0.0, all = 0.0;
+        for (auto& s : b->impl.sims) {
+            if (s->prm.field_kind != FS_FIELD_DIRECT32C) continue;
+            band += s->field->band_pairs(s->st);
+            all += s->field->last_pairs;
+        }
+        *band_pairs = band;
+        *pairs = all;
+    });
+}
+
 fs_status fs_batch_stats(fs_batch* b, int* targets_per_thread, int* tiles_per_item, long long* graph_steps,
                          long long* plain_steps) {
     return fsb::guard([&] {

@@ -255,3 +255,22 @@ def test_relativistic_member_alone_and_in_batch_bit_identical():
             assert np.array_equal(b2.state(a)[k], b3.state(c)[k]), k
     for b in (b1, b2, b3):
         b.close()
+
+
+def test_band_pairs_of_the_last_evaluation():
+    """fs_batch_band_pairs: the FP32c members' last evaluation counts n^2 pairs
+    each, of which the band |d| <= 16 eps (evaluated in FP64) is close to its
+    share 32 eps / L of a near-uniform Landau density; an FP64 member counts
+    none."""
+    ds = _small_decks(3, seed=5)
+    b = fs.Batch()
+    ids = [b.add(d) for d in ds]
+    b.add(ds[0], "direct64")
+    b.step(1)  # no remesh: the last evaluation is a full one
+    band, pairs = b.band_pairs()
+    ns = [b.info(i)["n"] for i in ids]
+    b.close()
+    assert pairs == float(sum(n * n for n in ns))
+    want = sum(n * n * 32 * d["greens_epsilon"] / (d["xmax"] - d["xmin"]) for n, d in zip(ns, ds))
+    assert 0 < band < pairs
+    assert abs(band / want - 1) < 0.3, (band, want)
