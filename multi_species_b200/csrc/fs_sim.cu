@@ -1162,6 +1162,27 @@ struct Sim {
         return ux;
     }
 
+    // Load the remesh kernels on this device at creation: with the CUDA
+    // runtime's lazy module loading the first remesh would otherwise pay for
+    // loading them (about 0.3-0.8 ms measured on a 0.4 ms remesh).
+    static void preload_remesh_kernels(int device) {
+        static std::mutex mu;
+        static std::vector<int> done;
+        std::lock_guard<std::mutex> lk(mu);
+        if (std::find(done.begin(), done.end(), device) != done.end()) return;
+        const void* fns[] = {(const void*)k_panel_fit,         (const void*)k_shift,
+                             (const void*)k_row_sort,          (const void*)k_leaf_xmid,
+                             (const void*)k_guess,             (const void*)k_walk_spec,
+                             (const void*)k_repair_column,     (const void*)k_repair_rows,
+                             (const void*)k_walk_first_column, (const void*)k_walk_rows,
+                             (const void*)k_eval_points,       (const void*)k_reset_points};
+        for (const void* f : fns) {
+            cudaFuncAttributes a;
+            FS_CUDA(cudaFuncGetAttributes(&a, f));
+        }
+        done.push_back(device);
+    }
+
     void create(const fs_sim_params& P, cudaStream_t external = nullptr) {
         prm = P;
         if (P.num_species < 1 || P.num_species > 8) fail(FS_ERR_ARG, "num_species must be 1..8");
@@ -1172,6 +1193,7 @@ struct Sim {
         if (P.use_external_field && (P.external_type < 0 || P.external_type > 2))
             fail(FS_ERR_ARG, "external_type must be 0 (tanh), 1 (sine) or 2 (logistic)");
         FS_CUDA(cudaSetDevice(P.device));
+        preload_remesh_kernels(P.device);
         if (external) {
             st = external;
             own_stream = false;
