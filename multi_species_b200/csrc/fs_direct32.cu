@@ -405,8 +405,12 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
             // and MUFU equally.  (One reciprocal per four targets -- 4.5
             // lane-ops and 0.25 MUFU per pair -- for 1/8 to 1/2 of the sources
             // measured 0.5-3.7% slower, and for 1, 2 or all 4 of a CTA's warps
-            // 3-4% slower.)  The FP32 sums are moved into the FP64
-            // accumulators every kFarChunk sources.
+            // 3-4% slower.  One or two of the four target pairs on the idle
+            // FP64 pipe instead, with a reciprocal from an integer seed and
+            // Newton steps, for every first, second or fourth source, measured
+            // 8-33% slower: 6.5 issue slots per pair there against 3.)  The
+            // FP32 sums are moved into the FP64 accumulators every kFarChunk
+            // sources.
             constexpr int kChunk = kFarChunk ? kFarChunk : kS;
 #pragma unroll 1
             for (int c = 0; c < kS; c += kChunk) {
@@ -434,6 +438,7 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
                     acc2[h] = make_float2(0.f, 0.f);
                 }
             }
+
         } else {
             // near band / image split: per-pair image and band; band pairs
             // q/2 * d / sqrt(d^2 + eps^2) in FP64 (as in band tiles), far pairs
