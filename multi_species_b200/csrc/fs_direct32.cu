@@ -253,6 +253,17 @@ static_assert(kFarChunk == 0 || (kFarChunk % 8 == 0 && 256 % kFarChunk == 0), "f
 #define FS_BAND_UNROLL 4
 #endif
 constexpr int kBandUnroll = FS_BAND_UNROLL;
+// far tiles: sources per unrolled body
+#ifndef FS_FAR_UNROLL
+#define FS_FAR_UNROLL 8
+#endif
+constexpr int kFarUnroll = FS_FAR_UNROLL;
+static_assert(kS % kFarUnroll == 0, "far unroll must divide the tile");
+// one simulation's persistent launch: about this many items per CTA
+#ifndef FS_ITEMS_PER_CTA
+#define FS_ITEMS_PER_CTA 32
+#endif
+constexpr int kItemsPerCta = FS_ITEMS_PER_CTA;
 // targets assigned contiguously per warp (1) or interleaved across the CTA (0)
 #ifndef FS_WARP_CONTIG
 #define FS_WARP_CONTIG 1
@@ -415,9 +426,9 @@ __device__ __forceinline__ bool pair_block(const PairJob& Jb, int tb, int chunk,
 #pragma unroll 1
             for (int c = 0; c < kS; c += kChunk) {
 #pragma unroll 1
-                for (int j0 = c; j0 < c + kChunk; j0 += 8) {
+                for (int j0 = c; j0 < c + kChunk; j0 += kFarUnroll) {
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
+                    for (int k = 0; k < kFarUnroll; ++k) {
                         const float4 e = tile[j0 + k];
                         const float2 sx2 = make_float2(e.x, e.x);
 #pragma unroll
@@ -812,7 +823,7 @@ class Direct32c final : public FieldEngine {
         const int nt_pad = (nt + kTBPad - 1) / kTBPad * kTBPad;
         const int tblocks = nt_pad / (kNT * R_);
         if (!grid_) grid_ = persistent_grid(R_);
-        const int want = grid_ * 32;
+        const int want = grid_ * kItemsPerCta;
         int nchunks = ntiles ? std::min(ntiles, std::max(1, (want + tblocks - 1) / tblocks)) : 1;
         const int tpc = ntiles ? (ntiles + nchunks - 1) / nchunks : 1;
         PairJob job;
