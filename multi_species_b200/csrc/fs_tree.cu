@@ -497,8 +497,14 @@ __global__ void k_far32(const TNode* __restrict__ nodes, const int* __restrict__
 // the kernel accumulates -+ lambda/2 c(v) (c = v/2 + v^2/8, v = eps^2 y^2).
 // Sources are staged through shared memory as FP32 offsets from an FP64 tile
 // base; each image's target offset is formed in FP64 before rounding.
-constexpr int kNearThreads = 128;
-constexpr int kNearR = 4;
+#ifndef FS_NEAR_THREADS
+#define FS_NEAR_THREADS 128
+#endif
+#ifndef FS_NEAR_R
+#define FS_NEAR_R 4
+#endif
+constexpr int kNearThreads = FS_NEAR_THREADS;
+constexpr int kNearR = FS_NEAR_R;
 constexpr int kNearBlock = kNearThreads * kNearR;
 constexpr int kNearTile = 256;
 constexpr double kNearBand = 24.0;
