@@ -289,6 +289,8 @@ def roofline(a, kern, kl, kms, kwork, total_ms, sm, peaks, peak_src, band_fracti
             "launches": kl, "avg_launch_ms": kms / kl if kl else None,
             "pairs_per_launch": kwork / kl if kl else None,
             "traffic": (tr["dram_bytes_per_pair"] * (kwork / kl)) if (tr and kl) else None,
+            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum per pair from profiles/"
+                               f"{tr['source']}, scaled by this run's pairs per launch") if tr else None,
             "kernel_share_of_step_time": kms / total_ms if total_ms else None}
     if a.field == "direct32c" and kern in ("k_pairs32", "k_pairs32_batched"):
         # far pairs on the FP32 pipe and MUFU, band pairs (|d| <= 16 eps) on
