@@ -863,8 +863,7 @@ class Direct32c final : public FieldEngine {
             k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout_.p, iout_.p, d_q, ns, ns_pad, e2 / 2,
                                                                  e2 * e2 / 8, src_.p, src64_.p, tbase_.p, qs_.p,
                                                                  qx_.p);
-            tb = cub_.bytes();
-            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb, qs_.p, pq_.p, ns, st));
+            scan_f64_inclusive(qs_.p, pq_.p, ns, scan_.p, st);
             tb = cub_.bytes();
             FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
             FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
@@ -952,6 +951,7 @@ class Direct32c final : public FieldEngine {
         qx_.ensure(ns);
         pq_.ensure(ns);
         qxsum_.ensure(1);
+        scan_.ensure(scan_f64_scratch(ns));
         tbase_.ensure(std::max(ntiles, 1));
         info_.ensure(nt_pad);
         partial_.ensure(npartial);
@@ -971,8 +971,6 @@ class Direct32c final : public FieldEngine {
         size_t need = 0, b = 0;
         FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (int*)nullptr,
                                                 (int*)nullptr, nsort, 0, 63));
-        need = std::max(need, b);
-        FS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, (double*)nullptr, (double*)nullptr, ns));
         need = std::max(need, b);
         FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, (double*)nullptr, (double*)nullptr, ns));
         need = std::max(need, b);
@@ -997,7 +995,7 @@ class Direct32c final : public FieldEngine {
     int last_nt_ = 0;
     DevBuf<int> cost_, ids_;
     DevBuf<unsigned char> ordtmp_;
-    DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_;
+    DevBuf<double> qs_, qx_, pq_, qxsum_, tbase_, partial_, scan_;
     DevBuf<TargetInfo> info_;
     DevBuf<int> err_, counter_;
     DevBuf<unsigned char> cub_;
@@ -1139,8 +1137,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     size_t need = 0, b = 0;
     FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, kin, kout, iin, iout, n, 0, 63));
     need = std::max(need, b);
-    FS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, qs, pq, n));
-    need = std::max(need, b);
+    need = std::max(need, scan_f64_scratch(n) * sizeof(double));
     FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, qx, qxsum, n));
     need = std::max(need, b);
     if (need > kNoAllocCubBytes) fail(FS_ERR_UNSUPPORTED, "sort scratch larger than the static reserve");
@@ -1153,8 +1150,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     const double e2 = eps * eps;
     k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, src64,
                                                          tbase, qs, qx);
-    tb = kNoAllocCubBytes;
-    FS_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp, tb, qs, pq, n, st));
+    scan_f64_inclusive(qs, pq, n, reinterpret_cast<double*>(cub_tmp), st);  // the sort is done with cub_tmp
     tb = kNoAllocCubBytes;
     FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);

@@ -268,6 +268,12 @@ int pairs_batched_grid(int R);
 // work of each (tiles x targets), appended to `items` / `cost`.
 void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>& items, std::vector<double>& cost);
 
+// Inclusive prefix sum of n doubles with a fixed association, so that its
+// results are the same on every run (csrc/fs_scan.cu); `scratch` holds
+// scan_f64_scratch(n) doubles.
+size_t scan_f64_scratch(int n);
+void scan_f64_inclusive(const double* in, double* out, int n, double* scratch, cudaStream_t st);
+
 // Polls of the pair kernels' tile waits on the current device (< 0: the
 // default bound); a test hook behind fs_debug_set_wait_limits.
 void set_mbar_polls(long long polls);

@@ -277,6 +277,10 @@ __global__ void k_item_counts(const TNode* __restrict__ nodes, const int* __rest
 // Partial moments of a member chunk of one node, one CTA per work item
 // (grid-stride over the items).  Per point the reference's arithmetic
 // (alloc_set_cluster_list :826-860) with one rounding per operation.
+// kPP > 0 fixes the number of Chebyshev nodes (degree + 1) at compile time, so
+// that the per-point arrays live in registers (with kPP = 0, read from P at
+// run time, they sit in local memory); the arithmetic is the same either way.
+template <int kPP>
 __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ nodes, const int* __restrict__ meta,
                                                       int cap_nodes, const int* __restrict__ item_start,
                                                       int cap_items, int P, const double* __restrict__ consts,
@@ -288,7 +292,7 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
                                          (nodes[nnodes - 1].m1 - nodes[nnodes - 1].m0 + kChunk) / kChunk);
     const double* cheb = consts;
     const double* wk = consts + (kMaxDegree + 1);
-    const int PP = P + 1;
+    const int PP = kPP > 0 ? kPP : P + 1;
     __shared__ double red[8 * (kMaxDegree + 1)];  // per warp (256 threads), per moment
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
         // node owning this item: last node with item_start <= item (nodes 1..nnodes-1)
@@ -303,6 +307,7 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
         const int a = nd.m0 + chunk * kChunk;
         const int e = min(nd.m1, a + kChunk - 1);
         double t[kMaxDegree + 1], acc[kMaxDegree + 1];
+#pragma unroll
         for (int k = 0; k < PP; ++k) {
             t[k] = dadd(nd.x0, dmul(dmul(dadd(cheb[k], 1.0), 0.5), dsub(nd.x1, nd.x0)));
             acc[k] = 0.0;
@@ -317,6 +322,7 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
             // between the spacing of doubles near x and the node width, so the
             // product neither underflows nor overflows)
             int k = 0;
+#pragma unroll
             for (; k + 1 < PP; k += 2) {
                 const double da = dsub(x, t[k]), db = dsub(x, t[k + 1]);
                 if (fabs(da) <= DBL_MIN || fabs(db) <= DBL_MIN) {
@@ -353,17 +359,19 @@ __global__ void __launch_bounds__(256) k_moment_items(const TNode* __restrict__ 
             }
             if (exact > -1) {
                 sum = 1.0;
-                for (int k = 0; k < PP; ++k) ak[k] = 0.0;
-                ak[exact] = 1.0;
+#pragma unroll
+                for (int k = 0; k < PP; ++k) ak[k] = (k == exact) ? 1.0 : 0.0;
             }
             const double D = ddiv(1.0, sum);
             const double l = lam[j];
+#pragma unroll
             for (int k = 0; k < PP; ++k) acc[k] = dadd(acc[k], dmul(dmul(ak[k], D), l));
         }
         // block reduction of PP values in a fixed order: a shuffle tree within
         // each warp, then the eight warp sums in warp order
         double* out = partial + (size_t)item * (kMaxDegree + 1);
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
         for (int k = 0; k < PP; ++k) {
             double v = acc[k];
 #pragma unroll
@@ -455,6 +463,11 @@ __global__ void k_far_near64(const TNode* __restrict__ nodes, const int* __restr
 
 // FP32-compensated form, far part: FP64 with the kernel written through one
 // reciprocal square root, K_tc(d) = norm * (d / (2 sqrt(d^2+eps^2)) - c d).
+#ifndef FS_FAR32_FAST
+#define FS_FAR32_FAST 0
+#endif
+constexpr bool kFar32Fast = FS_FAR32_FAST;
+
 __global__ void k_far32(const TNode* __restrict__ nodes, const int* __restrict__ meta, const int* __restrict__ leaf_of,
                         const int* __restrict__ far_list, const int* __restrict__ far_n,
                         const double* __restrict__ mom, const double* __restrict__ consts,
@@ -467,6 +480,7 @@ __global__ void k_far32(const TNode* __restrict__ nodes, const int* __restrict__
     const int l = leaf_of[j];
     const double x = sx[j];
     const double e2 = eps * eps;
+    const double invL = 1.0 / L;
     double far = 0.0;
     for (int f = 0; f < far_n[l]; ++f) {
         const int fi = far_list[(size_t)l * kFarCap + f];
@@ -475,8 +489,19 @@ __global__ void k_far32(const TNode* __restrict__ nodes, const int* __restrict__
         for (int k = 0; k < PP; ++k) {
             const double t = nd.x0 + (cheb[k] + 1.0) * 0.5 * (nd.x1 - nd.x0);
             double d = x - t;
-            d -= L * rint(d / L);
-            far += m[k] * (d * (0.5 * rsqrt(d * d + e2) - cbg));
+            if (kFar32Fast) {
+                // nearest image by a product with 1/L, 1/sqrt from the hardware
+                // approximation and one Newton step (relative error ~1e-14)
+                d -= L * rint(d * invL);
+                const double r = d * d + e2;
+                double y;
+                asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(r));
+                y = y * fma(-0.5 * r, y * y, 1.5);
+                far += m[k] * (d * (0.5 * y - cbg));
+            } else {
+                d -= L * rint(d / L);
+                far += m[k] * (d * (0.5 * rsqrt(d * d + e2) - cbg));
+            }
         }
     }
     efar[j] = norm * far;
@@ -760,6 +785,28 @@ __global__ void k_copy_meta_error(const int* __restrict__ meta, int* __restrict_
     if (meta[2]) atomicCAS(err, 0, meta[2]);
 }
 
+// k_moment_items for PP = degree + 1 Chebyshev nodes: compiled for each
+// supported node count, so that its per-point arrays stay in registers.
+void launch_moment_items(int PP, int grid, cudaStream_t st, const TNode* nodes, const int* meta, int cap_nodes,
+                         const int* item_start, int cap_items, int P, const double* consts, const double* sx,
+                         const double* lam, double* partial) {
+#define FS_MOMENT_CASE(n)                                                                                         \
+    case n:                                                                                                      \
+        k_moment_items<n><<<grid, 256, 0, st>>>(nodes, meta, cap_nodes, item_start, cap_items, P, consts, sx, lam, \
+                                                partial);                                                        \
+        break;
+    switch (PP) {
+        FS_MOMENT_CASE(2) FS_MOMENT_CASE(3) FS_MOMENT_CASE(4) FS_MOMENT_CASE(5) FS_MOMENT_CASE(6)
+        FS_MOMENT_CASE(7) FS_MOMENT_CASE(8) FS_MOMENT_CASE(9) FS_MOMENT_CASE(10) FS_MOMENT_CASE(11)
+        FS_MOMENT_CASE(12) FS_MOMENT_CASE(13) FS_MOMENT_CASE(14) FS_MOMENT_CASE(15) FS_MOMENT_CASE(16)
+        FS_MOMENT_CASE(17)
+        default:
+            k_moment_items<0><<<grid, 256, 0, st>>>(nodes, meta, cap_nodes, item_start, cap_items, P, consts, sx, lam,
+                                                    partial);
+    }
+#undef FS_MOMENT_CASE
+}
+
 class Treecode final : public FieldEngine {
    public:
     Treecode(double L, double eps, double mac, int degree, int max_source, bool fp32_near)
@@ -823,8 +870,8 @@ class Treecode final : public FieldEngine {
         k_item_counts<<<(cap_nodes + T - 1) / T, T, 0, st>>>(nodes_.p, meta_.p, cap_nodes, counts_.p);
         tb = cub_.bytes();
         FS_CUDA(cub::DeviceScan::ExclusiveSum(cub_.p, tb, counts_.p, item_start_.p, cap_nodes, st));
-        k_moment_items<<<sm_count() * 8, 256, 0, st>>>(nodes_.p, meta_.p, cap_nodes, item_start_.p, cap_items, P_,
-                                                       consts_.p, sx_.p, lam_.p, mpart_.p);
+        launch_moment_items(P_ + 1, sm_count() * 8, st, nodes_.p, meta_.p, cap_nodes, item_start_.p, cap_items, P_,
+                            consts_.p, sx_.p, lam_.p, mpart_.p);
         k_moment_reduce<<<(cap_nodes + T - 1) / T, T, 0, st>>>(nodes_.p, meta_.p, cap_nodes, item_start_.p, P_,
                                                               mpart_.p, mom_.p);
         k_copy_meta_error<<<1, 1, 0, st>>>(meta_.p, err_.p);
@@ -842,11 +889,9 @@ class Treecode final : public FieldEngine {
             }
             // leaves hold < max_source points: at most ceil(max_source/kNearBlock) target blocks each
             dim3 grid(cap_leaves, (N0_ + kNearBlock - 1) / kNearBlock);
-            size_t tb2 = cub_.bytes();
-            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb2, lam_.p, pl_.p, n, st));
+            scan_f64_inclusive(lam_.p, pl_.p, n, scan_.p, st);
             k_mul<<<(n + T - 1) / T, T, 0, st>>>(lam_.p, sx_.p, n, lx_.p);
-            tb2 = cub_.bytes();
-            FS_CUDA(cub::DeviceScan::InclusiveSum(cub_.p, tb2, lx_.p, plx_.p, n, st));
+            scan_f64_inclusive(lx_.p, plx_.p, n, scan_.p, st);
             ProfScope prof("k_near32", st, last_pairs);
             k_near32<<<grid, kNearThreads, 0, st>>>(nodes_.p, meta_.p, leaves_.p, near_.p, near_n_.p, sx_.p,
                                                    lam_.p, pl_.p, plx_.p, efar_.p, iout_.p, L_, eps_, cbg_, norm_,
@@ -870,6 +915,7 @@ class Treecode final : public FieldEngine {
             pl_.ensure(n);
             plx_.ensure(n);
             lx_.ensure(n);
+            scan_.ensure(scan_f64_scratch(n));
         }
         nodes_.ensure(cap_nodes);
         leaves_.ensure(cap_leaves);
@@ -893,8 +939,6 @@ class Treecode final : public FieldEngine {
         need = std::max(need, b);
         FS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, cap_nodes));
         need = std::max(need, b);
-        FS_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b, (double*)nullptr, (double*)nullptr, n));
-        need = std::max(need, b);
         cub_.ensure(need);
     }
 
@@ -904,7 +948,7 @@ class Treecode final : public FieldEngine {
     double norm_ = 1, cbg_ = 0;
     DevBuf<uint64_t> kin_, kout_;
     DevBuf<int> iin_, iout_, leaf_of_, leaves_, meta_, far_, far_n_, near_, near_n_, counts_, item_start_, err_;
-    DevBuf<double> sx_, lam_, efar_, mpart_, mom_, consts_, pl_, plx_, lx_, work_;
+    DevBuf<double> sx_, lam_, efar_, mpart_, mom_, consts_, pl_, plx_, lx_, work_, scan_;
     int cap_leaves_ = 0;
     DevBuf<TNode> nodes_;
     DevBuf<unsigned char> cub_;
