@@ -72,7 +72,8 @@ fs_status fs_field_destroy(fs_field* field);
  * arrays, synchronous.  Fully overwrites es[0..nt) (undefined when the call
  * returns an error).  For the treecode kinds the
  * reference ignores targets/nt and writes es[0..ns); so does this call
- * (nt must equal ns). */
+ * (nt must equal ns).  Every kind is deterministic: the same inputs on the
+ * same device give bit-identical es on every call. */
 fs_status fs_field_eval(fs_field* field, double* es, const double* targets, int nt,
                         const double* sources, const double* q_ws, int ns);
 

@@ -516,10 +516,17 @@ __global__ void __launch_bounds__(kNT) k_pairs32(PairJob job, int* __restrict__ 
 }
 
 // Many jobs (one per simulation of a batch), persistent: a fixed grid of CTAs
-// takes (job, target block, chunk) items from an atomic counter; items are
-// ordered longest first.
+// takes (job, target block, chunk) items from an atomic counter, in the order
+// `order` gives (band-heavy items spread over the queue) or the host's order
+// (longest first) when it is null.
+// CTAs per SM (in 64-thread units) the batched kernel is compiled for: 16 at
+// 4 targets per thread (64 registers; measured 4% faster than 12 CTAs at 80
+// registers on the 64-instance batch), 8 at 8 targets (128 registers, no spills)
+#ifndef FS_BATCH_MIN_BLOCKS4
+#define FS_BATCH_MIN_BLOCKS4 16
+#endif
 template <int kR>
-__global__ void __launch_bounds__(kNT) k_pairs32_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items,
+__global__ void __launch_bounds__(kNT, (kR >= 8 ? 8 : FS_BATCH_MIN_BLOCKS4) * 64 / kNT) k_pairs32_batched(const PairJob* __restrict__ jobs, const int4* __restrict__ items,
                                                          int nitems, const int* __restrict__ order,
                                                          int* __restrict__ counter, int* __restrict__ err) {
     __shared__ __align__(128) float4 buf[2][kS];
@@ -864,9 +871,8 @@ class Direct32c final : public FieldEngine {
                                                                  e2 * e2 / 8, src_.p, src64_.p, tbase_.p, qs_.p,
                                                                  qx_.p);
             scan_f64_inclusive(qs_.p, pq_.p, ns, scan_.p, st);
-            tb = cub_.bytes();
-            FS_CUDA(cub::DeviceReduce::Sum(cub_.p, tb, qx_.p, qxsum_.p, ns, st));
-            FS_LAUNCHED(2);  // own kernels (the sort / scan / reduce kernels are CUB's)
+            sum_f64(qx_.p, ns, scan_.p, qxsum_.p, st);
+            FS_LAUNCHED(2);  // k_wrap_keys, k_gather_sources (the sort is CUB's; the scan and sum count themselves)
         }
         const uint64_t* tkeys;
         const int* tperm;
@@ -971,8 +977,6 @@ class Direct32c final : public FieldEngine {
         size_t need = 0, b = 0;
         FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (int*)nullptr,
                                                 (int*)nullptr, nsort, 0, 63));
-        need = std::max(need, b);
-        FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, (double*)nullptr, (double*)nullptr, ns));
         need = std::max(need, b);
         cub_.ensure(need);
     }
@@ -1138,8 +1142,6 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     FS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b, kin, kout, iin, iout, n, 0, 63));
     need = std::max(need, b);
     need = std::max(need, scan_f64_scratch(n) * sizeof(double));
-    FS_CUDA(cub::DeviceReduce::Sum(nullptr, b, qx, qxsum, n));
-    need = std::max(need, b);
     if (need > kNoAllocCubBytes) fail(FS_ERR_UNSUPPORTED, "sort scratch larger than the static reserve");
 
     FS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
@@ -1151,8 +1153,7 @@ void direct32c_noalloc(double L, double eps, double* d_es, const double* d_x, co
     k_gather_sources<<<(ns_pad + T - 1) / T, T, 0, st>>>(kout, iout, d_q, n, ns_pad, e2 / 2, e2 * e2 / 8, src, src64,
                                                          tbase, qs, qx);
     scan_f64_inclusive(qs, pq, n, reinterpret_cast<double*>(cub_tmp), st);  // the sort is done with cub_tmp
-    tb = kNoAllocCubBytes;
-    FS_CUDA(cub::DeviceReduce::Sum(cub_tmp, tb, qx, qxsum, n, st));
+    sum_f64(qx, n, reinterpret_cast<double*>(cub_tmp), qxsum, st);
     k_target_info<<<(nt_pad + T - 1) / T, T, 0, st>>>(kout, n, nt_pad, kout, n, L, kBand * eps, pq, info);
     const PairJob job{src, src64, tbase, info, partial, n, ntiles, tpc, nt_pad, L, (float)e2, (float)(e2 / 2),
                       (float)(e2 * e2 / 8), (float)(0.75 * e2), e2, n};

@@ -273,6 +273,8 @@ void pair_job_items(const PairJob& job, int job_index, int R, std::vector<int4>&
 // scan_f64_scratch(n) doubles.
 size_t scan_f64_scratch(int n);
 void scan_f64_inclusive(const double* in, double* out, int n, double* scratch, cudaStream_t st);
+// out[0] = sum of in[0..n), with the same fixed association (same scratch).
+void sum_f64(const double* in, int n, double* scratch, double* out, cudaStream_t st);
 
 // Polls of the pair kernels' tile waits on the current device (< 0: the
 // default bound); a test hook behind fs_debug_set_wait_limits.

@@ -1,4 +1,4 @@
-// Deterministic inclusive prefix sum of doubles (sm_100a).
+// Deterministic inclusive prefix sum and sum of doubles (sm_100a).
 //
 // The field kernels form exact-in-FP64 sign sums and background terms from
 // prefix sums of the sorted charges.  A single-pass scan with decoupled
@@ -9,7 +9,8 @@
 // left to right, threads combined by a Kogge-Stone scan inside each warp and
 // across the warps, blocks by one block scanning the block totals the same way.
 // Three launches: block totals, their scan, and the final pass that rescans
-// each block from its offset.
+// each block from its offset.  sum_f64 is the same first pass and one CTA
+// summing the block totals.
 #include "fs_device.cuh"
 
 namespace fsb {
@@ -98,7 +99,31 @@ __global__ void __launch_bounds__(kScanT) k_scan_final(const double* __restrict_
     }
 }
 
+// One CTA: out[0] = the sum of bsum[0..nb), in a fixed association.
+__global__ void __launch_bounds__(kScanT) k_sum_totals(const double* __restrict__ bsum, int nb,
+                                                        double* __restrict__ out) {
+    __shared__ double sh[2 * kScanWarps];
+    const int per = (nb + kScanT - 1) / kScanT;
+    const int a = threadIdx.x * per, e = min(nb, a + per);
+    double s = 0.0;
+    for (int i = a; i < e; ++i) s += bsum[i];
+    double total;
+    (void)block_scan_excl(s, sh, &total);
+    if (threadIdx.x == 0) out[0] = total;
+}
+
 }  // namespace
+
+void sum_f64(const double* in, int n, double* scratch, double* out, cudaStream_t st) {
+    if (n <= 0) {
+        FS_CUDA(cudaMemsetAsync(out, 0, sizeof(double), st));
+        return;
+    }
+    const int nb = (n + kScanSeg - 1) / kScanSeg;
+    k_scan_totals<<<nb, kScanT, 0, st>>>(in, n, scratch);
+    k_sum_totals<<<1, kScanT, 0, st>>>(scratch, nb, out);
+    FS_LAUNCHED(2);
+}
 
 size_t scan_f64_scratch(int n) { return (size_t)std::max(1, (n + kScanSeg - 1) / kScanSeg); }
 
