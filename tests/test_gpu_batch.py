@@ -274,3 +274,29 @@ def test_band_pairs_of_the_last_evaluation():
     want = sum(n * n * 32 * d["greens_epsilon"] / (d["xmax"] - d["xmin"]) for n, d in zip(ns, ds))
     assert 0 < band < pairs
     assert abs(band / want - 1) < 0.3, (band, want)
+
+
+def test_large_members_take_the_ordered_launch_bit_identical_and_accurate():
+    """Members of 70k-200k points with 8 tiles per item give each batched launch
+    far more items than the persistent grid has CTAs, so the items are taken in
+    the device-computed order (band-heavy ones spread over the queue), which
+    depends on the whole mix.  A member's results are still bit-identical alone
+    and in the mix, and its field is within the error model of the FP64 sum."""
+    ds = [d for d in decks.landau_batch(count=64, seed=0, steps=10) if decks.deck_points(d) >= 70_000][:3]
+    assert len(ds) == 3
+    b1 = fs.Batch(tuning=(4, 8))
+    i1 = b1.add(ds[0])
+    b1.step(2)
+    alone = b1.state(i1)
+    b1.close()
+    b2 = fs.Batch(tuning=(4, 8))
+    ids = [b2.add(d) for d in ds]
+    b2.step(2)
+    mixed = [b2.state(i) for i in ids]
+    b2.close()
+    for k in alone:
+        assert np.array_equal(alone[k], mixed[0][k]), k
+    for d, st in zip(ds, mixed):
+        L = d["xmax"] - d["xmin"]
+        e64 = fs.E_MQ_DirectSum_B200(L, d["greens_epsilon"], "fp64").evaluate(st["xs"], st["xs"], st["q_ws"])
+        assert np.linalg.norm(st["es"] - e64) <= fp32c_bound(st["xs"], st["q_ws"], L, d["greens_epsilon"], e64)
