@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 shadow run (accuracy, plain FP64 rate)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch record")
+    ap.add_argument("--no-treecode", action="store_true",
+                    help="skip the full-size treecode record (also skipped with --no-accuracy)")
     ap.add_argument("--drift-steps", type=int, default=None,
                     help="steps of the FP32c-vs-FP64 field-energy comparison (default: warmup + steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -404,6 +406,8 @@ def run_ours(a, rank, world, local_rank):
             res["speedup_vs_plain_fp64_gpu"] = value / acc["plain_fp64_gpu"]["value"]
         if not a.no_batch and a.workload == "two_stream":
             res["batch"] = batch_summary(local_rank, a.batch, 2, 4)
+        if not a.no_treecode and not a.no_accuracy and a.workload == "two_stream":
+            res["treecode"] = treecode_summary(local_rank, 1, 3)
         if not a.no_e2e:
             res["e2e"] = e2e_plugin(deck, a.field, n, local_rank, a.steps)
         if not a.no_cpu_baseline:
@@ -521,6 +525,49 @@ def accuracy_vs_fp64(a, deck, local_rank, steps, sm, peaks):
                                             f"{DIRECT64_FP64_INSTR_PER_PAIR} FP64-pipe instructions per pair "
                                             "(ncu count, profiles/k_direct64_two_stream.md)"}
     return {"accuracy": acc, "plain_fp64_gpu": plain}
+
+
+def treecode_summary(local_rank, warmup, steps):
+    """Compact record of the treecode workload at full size (three species x
+    2,100,225 points, FP32c treecode, degree 8, theta 0.7, leaf 2000): step
+    time and pair rate over `steps` steps, and the final state's field
+    against the FP64 treecode (all targets) and against the plain FP64 direct
+    sum on 4096 evenly spaced targets (the treecode's own approximation)."""
+    import multi_species_b200 as M
+    from multi_species_b200 import decks
+    d = decks.bump_on_tail()
+    L = d["xmax"] - d["xmin"]
+    sim = M.Simulation(d, field_backend="treecode32c", device=local_rank)
+    sim.step(warmup)
+    p0, _ = sim.work()
+    ms = []
+    for _ in range(steps):
+        sim.step(1)
+        ms.extend(sim.step_times().tolist())
+    pairs = sim.work()[0] - p0
+    if sim.iteration()[0] % int(d["remesh_period"]) == 0:
+        sim.step(1)  # end on a full evaluation, not a remesh's reduced grid
+    st = sim.state()
+    sim.close()
+    x, q, e32 = st["xs"], st["q_ws"], st["es"]
+    f64 = M.E_MQ_Treecode_B200(L, d["greens_epsilon"], d["mac"], d["degree"], d["max_source"], precision="fp64",
+                               device=local_rank)
+    e64 = f64.evaluate(x, x, q)
+    f64.close()
+    idx = np.linspace(0, len(x) - 1, 4096).astype(np.int64)
+    fd = M.E_MQ_DirectSum_B200(L, d["greens_epsilon"], "fp64", device=local_rank)
+    ed = fd.evaluate(x[idx], x, q) * np.sqrt(L * L + 4 * d["greens_epsilon"] ** 2) / L
+    fd.close()
+    rel = lambda a_, b_: float(np.linalg.norm(a_ - b_) / np.linalg.norm(b_))
+    return {"workload": "bump_on_tail_treecode", "points": int(len(x)), "field": "treecode32c",
+            "steps": steps, "warmup": warmup, "ms_per_step": float(np.mean(ms)),
+            "value": pairs / (float(np.sum(ms)) / 1e3), "unit": "pair-interactions/s (direct-equivalent)",
+            "e_rel_l2_vs_fp64_treecode": rel(e32, e64),
+            "e_rel_l2_vs_fp64_direct_sampled": rel(e32[idx], ed),
+            "fp64_treecode_vs_fp64_direct_sampled": rel(e64[idx], ed),
+            "note": "all targets against the FP64 treecode; 4096 sampled targets against the FP64 direct sum "
+                    "(rescaled by the treecode kernel's sqrt(L^2 + 4 eps^2) / L), which measures the treecode's "
+                    "own approximation at theta 0.7, degree 8"}
 
 
 def batch_summary(local_rank, count, warmup, steps):
